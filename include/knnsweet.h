@@ -1,0 +1,152 @@
+/*
+ * knnsweet.h -- C ABI of the B200-native exact kNN join (libknnsweet.so).
+ *
+ * The reference (knn_sweet) has no library interface: its boundary is the
+ * `knnjoin` command line (src/knnjoin.cu:990-1001) over process globals
+ * (include/common8.h:14-24), and its result is the array
+ * `IndexDist knearest[query_nb*K]` (include/common8.h:37-40,
+ * src/knnjoin.cu:1104, 1139-1141): for every query, in the original query
+ * order, K pairs {source row index, Euclidean distance} in ascending distance.
+ * Each entry point below replaces one piece of that contract; the comment on
+ * each names the reference code it stands in for.
+ *
+ * Conventions
+ *  - Points are row-major float32, `d` floats per row, rows packed (stride d).
+ *  - Results are structure-of-arrays: out_idx[i*k + j] (int32, 0-based row of
+ *    the reference set) and out_dist[i*k + j] (float32 Euclidean distance),
+ *    j ascending by (squared distance, index): ties at equal distance go to the
+ *    lower reference index.  knn_pack_indexdist() converts to the reference's
+ *    interleaved {int index; float dist} layout.
+ *  - When fewer than k reference points exist (k > n), the missing slots hold
+ *    index -1 and distance +inf (the reference leaves them uninitialised).
+ *  - Every call returns 0 (KNN_OK) or a negative KNN_E* code and never exits
+ *    the process; knn_last_error() gives a message (per host thread).
+ *  - Calls hold no global state and may run concurrently from several host
+ *    threads; each call uses one CUDA stream.
+ */
+#ifndef KNNSWEET_H
+#define KNNSWEET_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KNNSWEET_ABI_VERSION 1
+
+/* Status codes (the reference prints and continues: src/knnjoin.cu:38-41). */
+#define KNN_OK 0
+#define KNN_EINVAL (-1)   /* bad argument: null pointer, d<=0, k<=0, sizes   */
+#define KNN_ENOMEM (-2)   /* a device or host allocation failed              */
+#define KNN_ECUDA (-3)    /* a CUDA runtime call or kernel launch failed     */
+#define KNN_ETIMEOUT (-4) /* a bounded device wait gave up                   */
+#define KNN_EINTERNAL (-5)/* a device-side consistency check failed          */
+
+/* Precision forms. */
+#define KNN_FP32 0        /* plain FP32 pruned join                          */
+#define KNN_BF16_REFINE 1 /* BF16 tensor-core distances, FP32 re-rank of the
+                             top k+margin, FP64 re-check of k-th ties         */
+
+/* Limits. */
+#define KNN_MAX_K 1024    /* the reference allows K <= 1000 (knnjoin.cu:774) */
+#define KNN_MAX_REPS 8192
+
+/*
+ * Options.  Defaults (knn_default_options): qreps = sreps = 0 meaning
+ * "choose from the set size" (about sqrt(n)*1.6, at most 4096; the reference
+ * takes them from argv[4], argv[5]: knnjoin.cu:997-998), seed = 2015
+ * (knnjoin.cu:199, 226), rep_trials = 10 (knnjoin.cu:195), precision = FP32,
+ * margin = 32, autotune = 1.
+ */
+typedef struct knn_options {
+  int32_t qreps;      /* number of query representatives (query clusters)    */
+  int32_t sreps;      /* number of reference representatives                 */
+  uint32_t seed;      /* glibc srand() seed used to draw representative rows */
+  int32_t rep_trials; /* random draws compared by pairwise spread            */
+  int32_t precision;  /* KNN_FP32 or KNN_BF16_REFINE                          */
+  int32_t margin;     /* extra candidates re-ranked by the BF16 form         */
+  int32_t autotune;   /* batched form: pick tiles per cloud-size bucket      */
+  int32_t flags;      /* reserved, must be 0                                 */
+} knn_options;
+
+/*
+ * Statistics of one call (the reference prints stage timers, common8.h:83-90,
+ * and the evaluation counter `Total`, knnjoin.cu:565-570, 804).
+ */
+typedef struct knn_stats {
+  int64_t dist_evals;       /* exact query-to-point distances evaluated       */
+  int64_t pairs_total;      /* m * n                                          */
+  int64_t pairs_pruned;     /* pairs_total - dist_evals                       */
+  int64_t clusters_visited; /* (query, reference cluster) pairs scanned        */
+  int64_t clusters_pruned;  /* (query, reference cluster) pairs skipped whole  */
+  int64_t refine_rechecks;  /* BF16 form: candidates re-checked in FP64        */
+  float ms_build;           /* representative sampling .. cluster filter      */
+  float ms_search;          /* per-query pruned scan                          */
+  float ms_total;           /* whole call, device time                        */
+  int32_t qreps_used;
+  int32_t sreps_used;
+  int32_t kernels_launched; /* device kernels this call enqueued (a radix sort
+                               counts as one)                                 */
+  int32_t reserved;
+} knn_stats;
+
+/* Fill `opt` with the defaults listed above. */
+void knn_default_options(knn_options *opt);
+
+/* Message for the last failing call on this host thread ("" if none). */
+const char *knn_last_error(void);
+
+/* ABI version (KNNSWEET_ABI_VERSION). */
+int32_t knn_abi_version(void);
+
+/*
+ * Exact kNN join on host buffers.  Replaces the whole reference pipeline
+ * main -> clusterReps -> RepsUpperBound -> FilterReps -> KNNQuery_base
+ * (src/knnjoin.cu:983-1145): copies q (m x d) and r (n x d) to the GPU, joins,
+ * and copies the m x k result back into out_idx / out_dist (host memory).
+ * `opt` may be NULL (defaults); `st` may be NULL.
+ */
+int knn_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d,
+             int32_t k, int32_t *out_idx, float *out_dist,
+             const knn_options *opt, knn_stats *st);
+
+/*
+ * Same join on device buffers (all four pointers are device memory of the
+ * current device), enqueued on `stream` (a cudaStream_t; NULL = legacy default
+ * stream).  Internal scratch comes from the stream-ordered allocator and is
+ * released before return.  Returns after enqueueing unless `st` is non-NULL,
+ * in which case it synchronises the stream to fill the statistics.
+ * q may equal r (self-join, as in run_sample.sh:1); then m must equal n.
+ */
+int knn_join_device(const float *q, int64_t m, const float *r, int64_t n,
+                    int32_t d, int32_t k, int32_t *out_idx, float *out_dist,
+                    const knn_options *opt, knn_stats *st, void *stream);
+
+/*
+ * Gradient of a loss over kNN pairs (no reference counterpart; the reference
+ * has no gradient).  For every pair (i, j=idx[i*k+t]) with upstream gradient
+ * g = grad_dist2[i*k+t] on the squared distance |q_i - r_j|^2:
+ *   grad_q[i] += 2 g (q_i - r_j),   grad_r[j] -= 2 g (q_i - r_j).
+ * Pairs with idx < 0 are skipped.  grad_q (m x d) and grad_r (n x d) are
+ * device buffers that are ACCUMULATED into (zero them first for a plain
+ * gradient); grad_r may be NULL.  Device pointers, enqueued on `stream`.
+ */
+int knn_backward_device(const float *q, int64_t m, const float *r, int64_t n,
+                        int32_t d, int32_t k, const int32_t *idx,
+                        const float *grad_dist2, float *grad_q, float *grad_r,
+                        void *stream);
+
+/*
+ * Interleave SoA results into the reference's IndexDist layout
+ * {int32 index; float dist} (include/common8.h:37-40), host memory,
+ * `count` = m * k entries.  out must hold 2*count 32-bit words.
+ */
+void knn_pack_indexdist(const int32_t *idx, const float *dist, int64_t count,
+                        void *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KNNSWEET_H */

@@ -1,0 +1,9 @@
+"""knn_sweet_b200: B200-native exact kNN join with triangle-inequality pruning.
+
+The compute path is libknnsweet.so (hand-written CUDA for sm_100a) behind the
+C ABI in include/knnsweet.h; this package is its Python front end.
+"""
+from ._lib import KnnError, load  # noqa: F401
+from .join import JoinStats, knnjoin, pack_indexdist  # noqa: F401
+
+__all__ = ["knnjoin", "pack_indexdist", "JoinStats", "KnnError", "load"]

@@ -1,0 +1,488 @@
+// api.cu -- orchestration of the exact kNN join and the C ABI entry points.
+//
+// Pipeline of one join (knn_join_device), all on one stream, no host round
+// trips after the representative draw:
+//   reference side: pack rows -> draw representatives (10 seeded trials,
+//     best spread) -> nearest representative per point -> one radix sort by
+//     (cluster, distance to representative) -> cluster-contiguous rows,
+//     member distances, offsets, min/max member distance
+//   query side: the same (shared with the reference side for a self-join)
+//   bounds: rep-rep distances -> per query cluster k-th upper bound and the
+//     surviving reference clusters, nearest first
+//   scan: one warp per query over its surviving clusters (scan.cu)
+// The reference runs the same stages with host sorts and per-cluster
+// device<->host copies in between (src/knnjoin.cu:166-411, 1043-1133).
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "glibc_rand.h"
+#include "kernels.cuh"
+
+namespace knnsweet {
+
+std::string &error_buffer() {
+  thread_local std::string s;
+  return s;
+}
+
+int &launch_counter() {
+  thread_local int n = 0;
+  return n;
+}
+
+void set_error(const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  error_buffer() = buf;
+}
+
+namespace {
+
+// Stream-ordered scratch: every allocation is released on the same stream
+// when the arena goes out of scope.
+class Arena {
+ public:
+  explicit Arena(cudaStream_t s) : s_(s) {}
+  ~Arena() {
+    for (void *p : ptrs_) cudaFreeAsync(p, s_);
+  }
+  Arena(const Arena &) = delete;
+  Arena &operator=(const Arena &) = delete;
+
+  template <class T>
+  int alloc(T **out, size_t count) {
+    *out = nullptr;
+    if (count == 0) count = 1;
+    void *p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, count * sizeof(T), s_);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      set_error("device allocation of %zu bytes failed: %s", count * sizeof(T),
+                cudaGetErrorString(e));
+      return e == cudaErrorMemoryAllocation ? KNN_ENOMEM : KNN_ECUDA;
+    }
+    ptrs_.push_back(p);
+    *out = static_cast<T *>(p);
+    return KNN_OK;
+  }
+
+ private:
+  cudaStream_t s_;
+  std::vector<void *> ptrs_;
+};
+
+#define KNN_TRY(expr)        \
+  do {                       \
+    int rc_ = (expr);        \
+    if (rc_ != KNN_OK) return rc_; \
+  } while (0)
+
+__global__ void fill_empty_kernel(int32_t *idx, float *dist, int64_t count) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    idx[t] = -1;
+    dist[t] = __int_as_float(0x7f800000);
+  }
+}
+
+// Small host arrays reach the device as kernel parameters (up to 8,000
+// words per launch): a pageable cudaMemcpyAsync would wait for the stream to
+// drain first, stalling back-to-back joins at every call.
+struct ParamChunk {
+  int32_t count;
+  int32_t v[8000];
+};
+
+__global__ void upload_kernel(int32_t *__restrict__ dst, const ParamChunk c) {
+  for (int i = threadIdx.x; i < c.count; i += blockDim.x) dst[i] = c.v[i];
+}
+
+int upload_i32(const std::vector<int32_t> &src, int32_t *dst, cudaStream_t s) {
+  ParamChunk c;
+  for (size_t base = 0; base < src.size(); base += 8000) {
+    size_t cnt = std::min<size_t>(8000, src.size() - base);
+    c.count = (int32_t)cnt;
+    memcpy(c.v, src.data() + base, cnt * sizeof(int32_t));
+    upload_kernel<<<1, 256, 0, s>>>(dst + base, c);
+    KNN_LAUNCH_CHECK();
+  }
+  return KNN_OK;
+}
+
+// Representative count when the caller passes 0: about 1.6 sqrt(n)
+// (the reference's sample run uses 800 for 145,057 points, run_sample.sh:1).
+int default_reps(int64_t n) {
+  double r = std::floor(1.6 * std::sqrt((double)n) + 0.5);
+  if (r < 1) r = 1;
+  if (r > 4096) r = 4096;
+  return (int)r;
+}
+
+// One clustered point set.
+struct ClusterSet {
+  int R = 0;
+  float4 *reps = nullptr;     // R x dp4s
+  int32_t *rep_rows = nullptr;
+  uint64_t *skeys = nullptr;  // n sorted (cluster, distance) keys
+  int32_t *perm = nullptr;    // sorted position -> input row
+  int32_t *off = nullptr;     // R + 1
+};
+
+int build_clusters(Arena &ar, const float4 *rows, int64_t n, int dp4s, int R,
+                   uint32_t seed, int trials, cudaStream_t s, ClusterSet *cs) {
+  cs->R = R;
+  // representative draw on the host: trials x R indices rand() % n
+  std::vector<int32_t> cand((size_t)trials * R);
+  GlibcRand g(seed);
+  for (auto &c : cand) c = g.next() % (int32_t)n;
+  int32_t *cand_dev;
+  uint32_t *score;
+  KNN_TRY(ar.alloc(&cand_dev, cand.size()));
+  KNN_TRY(ar.alloc(&score, (size_t)trials));
+  KNN_TRY(upload_i32(cand, cand_dev, s));
+  KNN_TRY(ar.alloc(&cs->reps, (size_t)R * dp4s));
+  KNN_TRY(ar.alloc(&cs->rep_rows, (size_t)R));
+  KNN_TRY(launch_rep_select(rows, dp4s, cand_dev, R, trials, score, cs->reps,
+                            cs->rep_rows, s));
+  int32_t *cl;
+  float *dr;
+  KNN_TRY(ar.alloc(&cl, (size_t)n));
+  KNN_TRY(ar.alloc(&dr, (size_t)n));
+  KNN_TRY(launch_assign(rows, n, dp4s, cs->reps, R, cl, dr, s));
+  uint64_t *keys;
+  int32_t *vals;
+  KNN_TRY(ar.alloc(&keys, (size_t)n));
+  KNN_TRY(ar.alloc(&vals, (size_t)n));
+  KNN_TRY(ar.alloc(&cs->skeys, (size_t)n));
+  KNN_TRY(ar.alloc(&cs->perm, (size_t)n));
+  size_t temp_bytes = cluster_sort_temp_bytes(n, R);
+  unsigned char *temp;
+  KNN_TRY(ar.alloc(&temp, temp_bytes));
+  KNN_TRY(launch_cluster_sort(cl, dr, n, R, keys, vals, cs->skeys, cs->perm, temp,
+                              temp_bytes, s));
+  KNN_TRY(ar.alloc(&cs->off, (size_t)R + 1));
+  KNN_TRY(launch_cluster_offsets(cs->skeys, n, R, cs->off, s));
+  return KNN_OK;
+}
+
+int check_options(const knn_options *opt, knn_options *o) {
+  knn_default_options(o);
+  if (opt) *o = *opt;
+  if (o->qreps < 0 || o->sreps < 0 || o->qreps > KNN_MAX_REPS ||
+      o->sreps > KNN_MAX_REPS) {
+    set_error("qreps/sreps must be in [0, %d]", KNN_MAX_REPS);
+    return KNN_EINVAL;
+  }
+  if (o->rep_trials <= 0 || o->rep_trials > 1000) {
+    set_error("rep_trials must be in [1, 1000]");
+    return KNN_EINVAL;
+  }
+  if (o->precision != KNN_FP32 && o->precision != KNN_BF16_REFINE) {
+    set_error("unknown precision %d", o->precision);
+    return KNN_EINVAL;
+  }
+  if (o->margin < 0 || o->margin > 4096) {
+    set_error("margin must be in [0, 4096]");
+    return KNN_EINVAL;
+  }
+  if (o->flags != 0) {
+    set_error("flags must be 0");
+    return KNN_EINVAL;
+  }
+  return KNN_OK;
+}
+
+int check_sizes(int64_t m, int64_t n, int32_t d, int32_t k) {
+  if (d <= 0) {
+    set_error("d must be positive (got %d)", d);
+    return KNN_EINVAL;
+  }
+  if (k <= 0 || k > KNN_MAX_K) {
+    set_error("k must be in [1, %d] (got %d)", KNN_MAX_K, k);
+    return KNN_EINVAL;
+  }
+  if (m < 0 || n < 0 || m > INT32_MAX || n > INT32_MAX) {
+    set_error("m and n must be in [0, 2^31-1]");
+    return KNN_EINVAL;
+  }
+  if (n > 0 && (int64_t)d > ((int64_t)1 << 40) / n) {
+    set_error("n * d too large");
+    return KNN_EINVAL;
+  }
+  return KNN_OK;
+}
+
+struct EventSet {
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  bool on = false;
+  ~EventSet() {
+    for (auto e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+  int create() {
+    for (auto &e : ev) KNN_CUDA_TRY(cudaEventCreate(&e));
+    on = true;
+    return KNN_OK;
+  }
+  int record(int i, cudaStream_t s) {
+    if (on) KNN_CUDA_TRY(cudaEventRecord(ev[i], s));
+    return KNN_OK;
+  }
+};
+
+int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
+                     int32_t d, int32_t k, int32_t *out_idx, float *out_dist,
+                     const knn_options *opt, knn_stats *st, cudaStream_t s) {
+  knn_options o;
+  KNN_TRY(check_options(opt, &o));
+  KNN_TRY(check_sizes(m, n, d, k));
+  if (st) memset(st, 0, sizeof *st);
+  launch_counter() = 0;
+  if (m == 0) return KNN_OK;
+  if (!q || !r || !out_idx || !out_dist) {
+    set_error("null pointer argument");
+    return KNN_EINVAL;
+  }
+  if (st) st->pairs_total = m * n;
+  if (n == 0) {
+    fill_empty_kernel<<<256, 256, 0, s>>>(out_idx, out_dist, m * (int64_t)k);
+    KNN_LAUNCH_CHECK();
+    return KNN_OK;
+  }
+  int dev = 0, num_sms = 148;
+  KNN_CUDA_TRY(cudaGetDevice(&dev));
+  KNN_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+
+  const int dp4 = (d + 3) / 4;
+  int dp4s = dp4, tmpl = 0;
+  if (dp4 <= 8) {
+    dp4s = 1;
+    while (dp4s < dp4) dp4s <<= 1;
+    tmpl = dp4s;
+  }
+  const bool self = (q == r) && (m == n);
+  int Rs = o.sreps > 0 ? o.sreps : default_reps(n);
+  int Rq = o.qreps > 0 ? o.qreps : (self ? Rs : default_reps(m));
+  if (Rs > n) Rs = (int)n;
+  if (Rq > m) Rq = (int)m;
+  const bool share = self && Rq == Rs;
+
+  EventSet evs;
+  if (st) KNN_TRY(evs.create());
+  KNN_TRY(evs.record(0, s));
+  Arena ar(s);
+
+  // packed rows (aliased when the input rows already are float4 rows)
+  auto packed = [&](const float *src, int64_t cnt, const float4 **outp) -> int {
+    if (dp4s * 4 == d && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+      *outp = reinterpret_cast<const float4 *>(src);
+      return KNN_OK;
+    }
+    float4 *p;
+    KNN_TRY(ar.alloc(&p, (size_t)cnt * dp4s));
+    KNN_TRY(launch_pack_rows(src, cnt, d, dp4s, p, s));
+    *outp = p;
+    return KNN_OK;
+  };
+  const float4 *Rp = nullptr, *Qp = nullptr;
+  KNN_TRY(packed(r, n, &Rp));
+  ClusterSet sset, qset;
+  KNN_TRY(build_clusters(ar, Rp, n, dp4s, Rs, o.seed, o.rep_trials, s, &sset));
+  float4 *srows;
+  float *sdist, *cmin, *cmax;
+  int32_t *sidx;
+  KNN_TRY(ar.alloc(&srows, (size_t)n * dp4s));
+  KNN_TRY(ar.alloc(&sdist, (size_t)n));
+  KNN_TRY(ar.alloc(&sidx, (size_t)n));
+  KNN_TRY(ar.alloc(&cmin, (size_t)Rs));
+  KNN_TRY(ar.alloc(&cmax, (size_t)Rs));
+  KNN_TRY(launch_cluster_layout(sset.skeys, sset.perm, n, Rp, dp4s, srows, sdist,
+                                sidx, s));
+  KNN_TRY(launch_cluster_minmax(sset.off, sdist, Rs, cmin, cmax, s));
+
+  if (share) {
+    Qp = Rp;
+    qset = sset;
+  } else {
+    KNN_TRY(packed(q, m, &Qp));
+    KNN_TRY(build_clusters(ar, Qp, m, dp4s, Rq, o.seed, o.rep_trials, s, &qset));
+  }
+  float *qrad, *drr, *theta0;
+  int32_t *slot_cl, *rlist, *rlen;
+  KNN_TRY(ar.alloc(&qrad, (size_t)Rq));
+  KNN_TRY(ar.alloc(&slot_cl, (size_t)m));
+  KNN_TRY(launch_query_clusters(qset.skeys, qset.off, m, Rq, qrad, slot_cl, s));
+  KNN_TRY(ar.alloc(&drr, (size_t)Rq * Rs));
+  KNN_TRY(launch_rep_dist(qset.reps, Rq, sset.reps, Rs, dp4s, drr, s));
+  KNN_TRY(ar.alloc(&theta0, (size_t)Rq));
+  KNN_TRY(ar.alloc(&rlist, (size_t)Rq * Rs));
+  KNN_TRY(ar.alloc(&rlen, (size_t)Rq));
+  KNN_TRY(launch_bounds_filter(drr, Rq, Rs, qrad, qset.off, sset.off, sdist, cmax,
+                               k, d, theta0, rlist, rlen, s));
+  KNN_TRY(evs.record(1, s));
+
+  unsigned long long *ctr;
+  KNN_TRY(ar.alloc(&ctr, 4));
+  KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, 4 * sizeof(unsigned long long), s));
+  ScanArgs a{};
+  a.qrows = Qp;
+  a.qorder = qset.perm;
+  a.slot_cl = slot_cl;
+  a.m = m;
+  a.d = d;
+  a.dp4 = dp4s;
+  a.dp4_tmpl = tmpl;
+  a.k = k;
+  a.sreps = sset.reps;
+  a.srows = srows;
+  a.sdist = sdist;
+  a.sidx = sidx;
+  a.soff = sset.off;
+  a.cmin = cmin;
+  a.cmax = cmax;
+  a.theta0 = theta0;
+  a.rlist = rlist;
+  a.rlen = rlen;
+  a.Rs = Rs;
+  a.out_idx = out_idx;
+  a.out_dist = out_dist;
+  a.work_counter = ctr;
+  a.counters = ctr + 1;
+  KNN_TRY(launch_scan(a, num_sms, s));
+  KNN_TRY(evs.record(2, s));
+
+  if (st) {
+    unsigned long long h[4];
+    KNN_CUDA_TRY(cudaMemcpyAsync(h, ctr, sizeof h, cudaMemcpyDeviceToHost, s));
+    KNN_CUDA_TRY(cudaStreamSynchronize(s));
+    st->dist_evals = (int64_t)h[1];
+    st->clusters_visited = (int64_t)h[2];
+    st->clusters_pruned = (int64_t)h[3];
+    st->pairs_pruned = st->pairs_total - st->dist_evals;
+    st->qreps_used = Rq;
+    st->sreps_used = Rs;
+    st->kernels_launched = launch_counter();
+    KNN_CUDA_TRY(cudaEventElapsedTime(&st->ms_build, evs.ev[0], evs.ev[1]));
+    KNN_CUDA_TRY(cudaEventElapsedTime(&st->ms_search, evs.ev[1], evs.ev[2]));
+    KNN_CUDA_TRY(cudaEventElapsedTime(&st->ms_total, evs.ev[0], evs.ev[2]));
+  }
+  return KNN_OK;
+}
+
+}  // namespace
+}  // namespace knnsweet
+
+using namespace knnsweet;
+
+extern "C" {
+
+void knn_default_options(knn_options *opt) {
+  if (!opt) return;
+  memset(opt, 0, sizeof *opt);
+  opt->qreps = 0;
+  opt->sreps = 0;
+  opt->seed = 2015;
+  opt->rep_trials = 10;
+  opt->precision = KNN_FP32;
+  opt->margin = 32;
+  opt->autotune = 1;
+  opt->flags = 0;
+}
+
+const char *knn_last_error(void) { return error_buffer().c_str(); }
+
+int32_t knn_abi_version(void) { return KNNSWEET_ABI_VERSION; }
+
+int knn_join_device(const float *q, int64_t m, const float *r, int64_t n,
+                    int32_t d, int32_t k, int32_t *out_idx, float *out_dist,
+                    const knn_options *opt, knn_stats *st, void *stream) {
+  error_buffer().clear();
+  return join_device_impl(q, m, r, n, d, k, out_idx, out_dist, opt, st,
+                          static_cast<cudaStream_t>(stream));
+}
+
+int knn_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d,
+             int32_t k, int32_t *out_idx, float *out_dist,
+             const knn_options *opt, knn_stats *st) {
+  error_buffer().clear();
+  {
+    knn_options o;
+    int rc = check_options(opt, &o);
+    if (rc != KNN_OK) return rc;
+    rc = check_sizes(m, n, d, k);
+    if (rc != KNN_OK) return rc;
+  }
+  if (m == 0) {
+    if (st) memset(st, 0, sizeof *st);
+    return KNN_OK;
+  }
+  if (!q || (!r && n > 0) || !out_idx || !out_dist) {
+    set_error("null pointer argument");
+    return KNN_EINVAL;
+  }
+  cudaStream_t s;
+  KNN_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  int rc = KNN_OK;
+  {
+    Arena ar(s);
+    const bool self = (q == r) && (m == n);
+    float *dq = nullptr, *dr = nullptr, *dd = nullptr;
+    int32_t *di = nullptr;
+    rc = ar.alloc(&dq, (size_t)m * d);
+    if (rc == KNN_OK && !self && n > 0) rc = ar.alloc(&dr, (size_t)n * d);
+    if (rc == KNN_OK) rc = ar.alloc(&di, (size_t)m * k);
+    if (rc == KNN_OK) rc = ar.alloc(&dd, (size_t)m * k);
+    if (self) dr = dq;
+    cudaError_t e = cudaSuccess;
+    if (rc == KNN_OK)
+      e = cudaMemcpyAsync(dq, q, sizeof(float) * m * d, cudaMemcpyHostToDevice, s);
+    if (rc == KNN_OK && e == cudaSuccess && !self && n > 0)
+      e = cudaMemcpyAsync(dr, r, sizeof(float) * n * d, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+      set_error("host-to-device copy failed: %s", cudaGetErrorString(e));
+      rc = KNN_ECUDA;
+    }
+    if (rc == KNN_OK)
+      rc = join_device_impl(dq, m, dr, n, d, k, di, dd, opt, st, s);
+    if (rc == KNN_OK) {
+      e = cudaMemcpyAsync(out_idx, di, sizeof(int32_t) * m * k,
+                          cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out_dist, dd, sizeof(float) * m * k,
+                            cudaMemcpyDeviceToHost, s);
+      if (e != cudaSuccess) {
+        set_error("device-to-host copy failed: %s", cudaGetErrorString(e));
+        rc = KNN_ECUDA;
+      }
+    }
+  }
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess && rc == KNN_OK) {
+    set_error("join failed on the device: %s", cudaGetErrorString(e));
+    rc = KNN_ECUDA;
+  }
+  cudaStreamDestroy(s);
+  return rc;
+}
+
+void knn_pack_indexdist(const int32_t *idx, const float *dist, int64_t count,
+                        void *out) {
+  if (!idx || !dist || !out) return;
+  uint32_t *o = static_cast<uint32_t *>(out);
+  for (int64_t i = 0; i < count; i++) {
+    uint32_t b;
+    memcpy(&b, dist + i, 4);
+    o[2 * i] = (uint32_t)idx[i];
+    o[2 * i + 1] = b;
+  }
+}
+
+}  // extern "C"

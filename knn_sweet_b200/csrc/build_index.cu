@@ -1,0 +1,556 @@
+// build_index.cu -- device-side index build of the pruned kNN join.
+//
+// Stages (each replaces the reference code cited on it):
+//   pack_rows_kernel       row-major input -> padded float4 rows
+//   rep_score_kernel       spread score of each random representative draw
+//   rep_pick_kernel        first best draw -> representative rows
+//   assign_kernel<DP4>     nearest representative + distance per point
+//   cluster_keys_kernel    (cluster, distance) sort keys
+//   cluster_layout_kernel  cluster-contiguous, distance-sorted copy of the rows
+//   cluster_bounds_kernel  cluster offsets, min/max member distance
+//   rep_dist_kernel        representative-to-representative distances
+//   bounds_filter_kernel   per query cluster: k-th upper bound + surviving
+//                          reference clusters sorted by rep-rep distance
+#include <cub/device/device_radix_sort.cuh>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace knnsweet {
+
+// ---------------------------------------------------------------------------
+// Row packing: n x d row-major floats -> n x dp4 float4 (zero padded).
+// ---------------------------------------------------------------------------
+__global__ void pack_rows_kernel(const float *__restrict__ src, int64_t n,
+                                 int d, int dp4, float4 *__restrict__ dst) {
+  int64_t total = n * dp4;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t row = t / dp4;
+    int c = (int)(t - row * dp4);
+    const float *s = src + row * d + 4 * c;
+    int rem = d - 4 * c;  // <= 0 for chunks past ceil(d/4) (power-of-2 width)
+    float4 v;
+    v.x = rem > 0 ? s[0] : 0.0f;
+    v.y = rem > 1 ? s[1] : 0.0f;
+    v.z = rem > 2 ? s[2] : 0.0f;
+    v.w = rem > 3 ? s[3] : 0.0f;
+    dst[t] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Representative draw (src/knnjoin.cu:125-154, host draw 195-239).
+// cand[t * R + i] are row indices drawn on the host with the glibc generator.
+// score[t] = wrapping int32 sum over ordered pairs (i, j) of (int)dist.
+// grid: (ceil(R / blockDim), trials)
+// ---------------------------------------------------------------------------
+__global__ void rep_score_kernel(const float4 *__restrict__ rows, int dp4,
+                                 const int32_t *__restrict__ cand, int R,
+                                 uint32_t *__restrict__ score) {
+  int t = blockIdx.y;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int32_t *c = cand + (int64_t)t * R;
+  uint32_t sum = 0;
+  if (i < R) {
+    const float4 *a = rows + (int64_t)c[i] * dp4;
+    for (int j = 0; j < R; j++) {
+      const float4 *b = rows + (int64_t)c[j] * dp4;
+      float dd = sqrtf(dist2_rows_rt(a, b, dp4));
+      sum += (uint32_t)(int32_t)dd;
+    }
+  }
+  // warp reduce then one atomic per warp (wrapping unsigned add)
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(score + t, sum);
+}
+
+// Picks the first trial whose score, compared as float against a running
+// best starting at 0.0f, is larger (selectReps_max, knnjoin.cu:135-148) and
+// gathers its rows.  One block.
+__global__ void rep_pick_kernel(const float4 *__restrict__ rows, int dp4,
+                                const int32_t *__restrict__ cand, int R,
+                                int trials, const uint32_t *__restrict__ score,
+                                float4 *__restrict__ reps,
+                                int32_t *__restrict__ rep_rows) {
+  __shared__ int best_s;
+  if (threadIdx.x == 0) {
+    float best = 0.0f;
+    int bt = 0;
+    for (int t = 0; t < trials; t++) {
+      float v = (float)(int32_t)score[t];
+      if (best < v) {
+        best = v;
+        bt = t;
+      }
+    }
+    best_s = bt;
+  }
+  __syncthreads();
+  const int32_t *c = cand + (int64_t)best_s * R;
+  for (int i = threadIdx.x; i < R; i += blockDim.x) {
+    int32_t row = c[i];
+    if (rep_rows) rep_rows[i] = row;
+    for (int k = 0; k < dp4; k++) reps[(int64_t)i * dp4 + k] = rows[(int64_t)row * dp4 + k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Nearest representative (findQCluster / findTCluster, knnjoin.cu:64-97):
+// argmin over representatives of the FP32 distance, lowest representative
+// index on ties.  The reference computes the distances as
+// sqrt(|x|^2 + |r|^2 - 2 x.r) through cuBLAS (knnjoin.cu:270-284, 55-63);
+// here they are computed directly, which cannot go negative.
+// Representatives are staged through shared memory in tiles.
+// ---------------------------------------------------------------------------
+template <int DP4>
+__global__ void __launch_bounds__(256)
+    assign_kernel(const float4 *__restrict__ rows, int64_t n,
+                  const float4 *__restrict__ reps, int R,
+                  int32_t *__restrict__ cl, float *__restrict__ dr) {
+  constexpr int TILE = (DP4 <= 2) ? 1024 : (DP4 <= 4 ? 512 : 256);
+  __shared__ float4 srep[TILE * DP4];
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  float4 p[DP4];
+#pragma unroll
+  for (int c = 0; c < DP4; c++)
+    p[c] = i < n ? rows[i * DP4 + c] : make_float4(0.f, 0.f, 0.f, 0.f);
+  // bi starts at 0 so that a point with a NaN coordinate (no comparison
+  // succeeds) still lands in a valid cluster.
+  float best = __int_as_float(0x7f7fffff);  // FLT_MAX
+  int bi = 0;
+  for (int base = 0; base < R; base += TILE) {
+    int cnt = min(TILE, R - base);
+    __syncthreads();
+    for (int t = threadIdx.x; t < cnt * DP4; t += blockDim.x)
+      srep[t] = reps[(int64_t)base * DP4 + t];
+    __syncthreads();
+    for (int j = 0; j < cnt; j++) {
+      float v = dist2_rows<DP4>(p, srep + j * DP4);
+      if (v < best) {
+        best = v;
+        bi = base + j;
+      }
+    }
+  }
+  if (i < n) {
+    cl[i] = bi;
+    dr[i] = sqrtf(best);
+  }
+}
+
+// Runtime-width variant for rows wider than 32 floats: the point row is read
+// through the read-only cache for every representative.
+__global__ void __launch_bounds__(256)
+    assign_kernel_rt(const float4 *__restrict__ rows, int64_t n, int dp4,
+                     const float4 *__restrict__ reps, int R,
+                     int32_t *__restrict__ cl, float *__restrict__ dr) {
+  extern __shared__ float4 srep_rt[];
+  const int TILE = 8192 / dp4 > 0 ? 8192 / dp4 : 1;  // 128 KB of float4
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const float4 *p = rows + (i < n ? i : 0) * dp4;
+  float best = __int_as_float(0x7f7fffff);
+  int bi = 0;
+  for (int base = 0; base < R; base += TILE) {
+    int cnt = min(TILE, R - base);
+    __syncthreads();
+    for (int t = threadIdx.x; t < cnt * dp4; t += blockDim.x)
+      srep_rt[t] = reps[(int64_t)base * dp4 + t];
+    __syncthreads();
+    for (int j = 0; j < cnt; j++) {
+      float v = dist2_rows_rt(p, srep_rt + j * dp4, dp4);
+      if (v < best) {
+        best = v;
+        bi = base + j;
+      }
+    }
+  }
+  if (i < n) {
+    cl[i] = bi;
+    dr[i] = sqrtf(best);
+  }
+}
+
+// Sort keys (cluster << 32 | distance bits) and identity values.
+__global__ void cluster_keys_kernel(const int32_t *__restrict__ cl,
+                                    const float *__restrict__ dr, int64_t n,
+                                    uint64_t *__restrict__ keys,
+                                    int32_t *__restrict__ vals) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    keys[i] = ((uint64_t)(uint32_t)cl[i] << 32) | __float_as_uint(dr[i]);
+    vals[i] = (int32_t)i;
+  }
+}
+
+// Cluster-contiguous layout: row p of the sorted set is input row perm[p];
+// its distance to the representative is the low word of its key.
+// (fillTMembers + host sort, knnjoin.cu:106-113, 382-399, without the
+// per-cluster device<->host round trips.)
+__global__ void cluster_layout_kernel(const uint64_t *__restrict__ skeys,
+                                      const int32_t *__restrict__ perm,
+                                      int64_t n, const float4 *__restrict__ rows,
+                                      int dp4, float4 *__restrict__ srows,
+                                      float *__restrict__ sdist,
+                                      int32_t *__restrict__ sidx) {
+  int64_t total = n * dp4;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t p = t / dp4;
+    int c = (int)(t - p * dp4);
+    int32_t src = perm[p];
+    srows[t] = rows[(int64_t)src * dp4 + c];
+    if (c == 0) {
+      if (sdist) sdist[p] = __uint_as_float((uint32_t)(skeys[p] & 0xffffffffu));
+      if (sidx) sidx[p] = src;
+    }
+  }
+}
+
+// Offsets of every cluster in the sorted order (off[R] = n) from the sorted
+// keys, plus min / max member distance (the reference never fills the
+// reference-cluster radius: knnjoin.cu:391, defect B1).
+__global__ void cluster_bounds_kernel(const uint64_t *__restrict__ skeys,
+                                      int64_t n, int R,
+                                      int32_t *__restrict__ off) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    int c = (int)(skeys[p] >> 32);
+    int prev = p == 0 ? -1 : (int)(skeys[p - 1] >> 32);
+    for (int x = prev + 1; x <= c; x++) off[x] = (int32_t)p;
+    if (p == n - 1)
+      for (int x = c + 1; x <= R; x++) off[x] = (int32_t)n;
+  }
+}
+
+__global__ void cluster_minmax_kernel(const int32_t *__restrict__ off,
+                                      const float *__restrict__ sdist, int R,
+                                      float *__restrict__ cmin,
+                                      float *__restrict__ cmax) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < R) {
+    int a = off[c], b = off[c + 1];
+    cmin[c] = b > a ? sdist[a] : 0.0f;
+    cmax[c] = b > a ? sdist[b - 1] : 0.0f;
+  }
+}
+
+// Same for clusters of the query set when only the maximum is needed
+// (maxquery, knnjoin.cu:78).
+__global__ void cluster_max_from_keys_kernel(const uint64_t *__restrict__ skeys,
+                                             const int32_t *__restrict__ off,
+                                             int R, float *__restrict__ cmax) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < R) {
+    int a = off[c], b = off[c + 1];
+    cmax[c] = b > a ? __uint_as_float((uint32_t)(skeys[b - 1] & 0xffffffffu)) : 0.0f;
+  }
+}
+
+// Cluster id of every query slot in the sorted query order.
+__global__ void slot_cluster_kernel(const uint64_t *__restrict__ skeys,
+                                    int64_t m, int32_t *__restrict__ slot_cl) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < m;
+       p += (int64_t)gridDim.x * blockDim.x)
+    slot_cl[p] = (int32_t)(skeys[p] >> 32);
+}
+
+// d(Rq_a, Rs_b) for all pairs (the reference recomputes these inside
+// RepsUpperBound and FilterReps: knnjoin.cu:468, 513).
+__global__ void rep_dist_kernel(const float4 *__restrict__ qreps, int Rq,
+                                const float4 *__restrict__ sreps, int Rs,
+                                int dp4, float *__restrict__ drr) {
+  int64_t total = (int64_t)Rq * Rs;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int a = (int)(t / Rs), b = (int)(t - (int64_t)a * Rs);
+    drr[t] = sqrtf(dist2_rows_rt(qreps + (int64_t)a * dp4, sreps + (int64_t)b * dp4, dp4));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Per query cluster (one block each):
+//  1. theta0 = k-th smallest over all reference points s of
+//     rq + d(Rq, Rs(s)) + d(s, Rs(s)), the bound RepsUpperBound computes
+//     (knnjoin.cu:459-504), found exactly by bisection on the value's bit
+//     pattern with a count of values <= T (binary search per cluster over its
+//     first min(k, size) members).  The reference keeps the K smallest in a
+//     list and replaces every entry equal to the maximum at once (486-489,
+//     defect B2), which undercounts ties; the count here is exact.  Widened
+//     by the rounding slack.
+//  2. The reference clusters Rs that can hold a point within theta0 of some
+//     query of the cluster: d(Rq,Rs) - rq - radius(Rs) <= theta0
+//     (FilterReps, knnjoin.cu:506-525), sorted by d(Rq,Rs), then Rs
+//     (the host std::sort of knnjoin.cu:1080-1091).
+// dynamic shared memory: RsPow2 * 8 bytes (sort keys).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(512)
+    bounds_filter_kernel(const float *__restrict__ drr, int Rq, int Rs,
+                         const float *__restrict__ qrad,
+                         const int32_t *__restrict__ qoff,
+                         const int32_t *__restrict__ soff,
+                         const float *__restrict__ sdist,
+                         const float *__restrict__ scmax, int k, int d,
+                         int rs_pow2, float *__restrict__ theta0,
+                         int32_t *__restrict__ rlist,
+                         int32_t *__restrict__ rlen) {
+  extern __shared__ uint64_t skey[];
+  __shared__ int red_i[32];
+  __shared__ unsigned red_u[32];
+  __shared__ int kept_s;
+  const int qc = blockIdx.x;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nth >> 5;
+  const float tol = bound_tol(d);
+  if (qoff[qc + 1] == qoff[qc]) {  // empty query cluster
+    if (tid == 0) {
+      theta0[qc] = 0.0f;
+      rlen[qc] = 0;
+    }
+    return;
+  }
+  const float rq = qrad[qc];
+  const float *dq = drr + (int64_t)qc * Rs;
+  const int64_t n = soff[Rs];
+  const int kk = (int)(k < n ? k : n);
+
+  // upper end of the bisection: the largest value any cluster contributes
+  unsigned hi_local = 0;
+  for (int j = tid; j < Rs; j += nth) {
+    int a = soff[j], sz = min(soff[j + 1] - a, kk);
+    if (sz > 0) {
+      float v = __fadd_rn(__fadd_rn(rq, dq[j]), sdist[a + sz - 1]);
+      hi_local = max(hi_local, __float_as_uint(v));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) hi_local = max(hi_local, __shfl_xor_sync(kFull, hi_local, o));
+  if (lane == 0) red_u[warp] = hi_local;
+  __syncthreads();
+  unsigned hi = 0;
+  for (int w = 0; w < nwarp; w++) hi = max(hi, red_u[w]);
+  __syncthreads();
+  // smallest bit pattern T with count(values <= T) >= kk; count(hi) >= kk.
+  unsigned lo = 0;  // count(lo - 1) < kk is implied for lo = 0
+  // invariant: answer in [lo, hi]
+  while (lo < hi) {
+    unsigned mid = lo + ((hi - lo) >> 1);
+    float T = __uint_as_float(mid);
+    int cnt = 0;
+    for (int j = tid; j < Rs; j += nth) {
+      int a = soff[j], sz = min(soff[j + 1] - a, kk);
+      if (sz == 0) continue;
+      float base = __fadd_rn(rq, dq[j]);
+      int l = 0, h = sz;  // first t with base + sdist[a+t] > T
+      while (l < h) {
+        int md = (l + h) >> 1;
+        if (__fadd_rn(base, sdist[a + md]) <= T) l = md + 1;
+        else h = md;
+      }
+      cnt += l;
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kFull, cnt, o);
+    if (lane == 0) red_i[warp] = cnt;
+    __syncthreads();
+    int total = 0;
+    for (int w = 0; w < nwarp; w++) total += red_i[w];
+    __syncthreads();
+    if (total >= kk) hi = mid;
+    else lo = mid + 1;
+  }
+  const float kth = __uint_as_float(hi);
+  const float th = __fmaf_rn(kth, 4.0f * tol, kth) + 1.17549435e-38f;
+  if (tid == 0) {
+    theta0[qc] = th;
+    kept_s = 0;
+  }
+  __syncthreads();
+
+  // filter + sort the survivors by (d(Rq,Rs), Rs)
+  for (int j = tid; j < rs_pow2; j += nth) {
+    uint64_t key = kKeyMax;
+    if (j < Rs && soff[j + 1] > soff[j]) {
+      float dd = dq[j], rr = scmax[j];
+      float lb = dd - rq - rr;
+      if (!(lb > th + tol * (dd + rq + rr + th))) {
+        key = ((uint64_t)__float_as_uint(dd) << 32) | (uint32_t)j;
+        atomicAdd(&kept_s, 1);
+      }
+    }
+    skey[j] = key;
+  }
+  __syncthreads();
+  for (int size = 2; size <= rs_pow2; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int t = tid; t < (rs_pow2 >> 1); t += nth) {
+        int i = 2 * t - (t & (stride - 1));
+        int j = i + stride;
+        bool up = (i & size) == 0;
+        uint64_t a = skey[i], b = skey[j];
+        if ((a > b) == up) {
+          skey[i] = b;
+          skey[j] = a;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  const int kept = kept_s;
+  for (int j = tid; j < kept; j += nth)
+    rlist[(int64_t)qc * Rs + j] = (int32_t)(skey[j] & 0xffffffffu);
+  if (tid == 0) rlen[qc] = kept;
+}
+
+// ---------------------------------------------------------------------------
+// Host-side launchers
+// ---------------------------------------------------------------------------
+static int grid_for(int64_t work, int threads) {
+  int64_t g = (work + threads - 1) / threads;
+  int64_t cap = 148LL * 32;
+  if (g > cap) g = cap;
+  return (int)(g < 1 ? 1 : g);
+}
+
+int launch_pack_rows(const float *src, int64_t n, int d, int dp4, float4 *dst,
+                     cudaStream_t s) {
+  if (n == 0) return KNN_OK;
+  pack_rows_kernel<<<grid_for(n * dp4, 256), 256, 0, s>>>(src, n, d, dp4, dst);
+  KNN_LAUNCH_CHECK();
+  return KNN_OK;
+}
+
+int launch_rep_select(const float4 *rows, int dp4, const int32_t *cand_dev,
+                      int R, int trials, uint32_t *score_dev, float4 *reps,
+                      int32_t *rep_rows, cudaStream_t s) {
+  KNN_CUDA_TRY(cudaMemsetAsync(score_dev, 0, sizeof(uint32_t) * trials, s));
+  dim3 grid((R + 127) / 128, trials);
+  rep_score_kernel<<<grid, 128, 0, s>>>(rows, dp4, cand_dev, R, score_dev);
+  KNN_LAUNCH_CHECK();
+  rep_pick_kernel<<<1, 256, 0, s>>>(rows, dp4, cand_dev, R, trials, score_dev,
+                                    reps, rep_rows);
+  KNN_LAUNCH_CHECK();
+  return KNN_OK;
+}
+
+int launch_assign(const float4 *rows, int64_t n, int dp4, const float4 *reps,
+                  int R, int32_t *cl, float *dr, cudaStream_t s) {
+  if (n == 0) return KNN_OK;
+  int blocks = (int)((n + 255) / 256);
+  switch (dp4) {
+#define KNN_ASSIGN_CASE(D)                                                   \
+  case D:                                                                    \
+    assign_kernel<D><<<blocks, 256, 0, s>>>(rows, n, reps, R, cl, dr);       \
+    break;
+    KNN_ASSIGN_CASE(1)
+    KNN_ASSIGN_CASE(2)
+    KNN_ASSIGN_CASE(3)
+    KNN_ASSIGN_CASE(4)
+    KNN_ASSIGN_CASE(5)
+    KNN_ASSIGN_CASE(6)
+    KNN_ASSIGN_CASE(7)
+    KNN_ASSIGN_CASE(8)
+#undef KNN_ASSIGN_CASE
+    default: {
+      int tile = 8192 / dp4 > 0 ? 8192 / dp4 : 1;
+      size_t smem = (size_t)tile * dp4 * sizeof(float4);
+      if (smem > 48 * 1024)
+        KNN_CUDA_TRY(cudaFuncSetAttribute(
+            assign_kernel_rt, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int)smem));
+      assign_kernel_rt<<<blocks, 256, smem, s>>>(rows, n, dp4, reps, R, cl, dr);
+    }
+  }
+  KNN_LAUNCH_CHECK();
+  return KNN_OK;
+}
+
+size_t cluster_sort_temp_bytes(int64_t n, int R) {
+  size_t bytes = 0;
+  int end_bit = 32;
+  while ((1LL << (end_bit - 32)) < (int64_t)R) end_bit++;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint64_t *)nullptr,
+                                  (uint64_t *)nullptr, (const int32_t *)nullptr,
+                                  (int32_t *)nullptr, (int)n, 0, end_bit);
+  return bytes;
+}
+
+int launch_cluster_sort(const int32_t *cl, const float *dr, int64_t n, int R,
+                        uint64_t *keys, int32_t *vals, uint64_t *skeys,
+                        int32_t *perm, void *temp, size_t temp_bytes,
+                        cudaStream_t s) {
+  if (n == 0) return KNN_OK;
+  cluster_keys_kernel<<<grid_for(n, 256), 256, 0, s>>>(cl, dr, n, keys, vals);
+  KNN_LAUNCH_CHECK();
+  int end_bit = 32;
+  while ((1LL << (end_bit - 32)) < (int64_t)R) end_bit++;
+  KNN_CUDA_TRY(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, skeys,
+                                               vals, perm, (int)n, 0, end_bit, s));
+  ++launch_counter();
+  return KNN_OK;
+}
+
+int launch_cluster_layout(const uint64_t *skeys, const int32_t *perm, int64_t n,
+                          const float4 *rows, int dp4, float4 *srows,
+                          float *sdist, int32_t *sidx, cudaStream_t s) {
+  if (n == 0) return KNN_OK;
+  cluster_layout_kernel<<<grid_for(n * dp4, 256), 256, 0, s>>>(
+      skeys, perm, n, rows, dp4, srows, sdist, sidx);
+  KNN_LAUNCH_CHECK();
+  return KNN_OK;
+}
+
+int launch_cluster_offsets(const uint64_t *skeys, int64_t n, int R, int32_t *off,
+                           cudaStream_t s) {
+  if (n == 0) {
+    KNN_CUDA_TRY(cudaMemsetAsync(off, 0, sizeof(int32_t) * (R + 1), s));
+    return KNN_OK;
+  }
+  cluster_bounds_kernel<<<grid_for(n, 256), 256, 0, s>>>(skeys, n, R, off);
+  KNN_LAUNCH_CHECK();
+  return KNN_OK;
+}
+
+int launch_cluster_minmax(const int32_t *off, const float *sdist, int R,
+                          float *cmin, float *cmax, cudaStream_t s) {
+  cluster_minmax_kernel<<<(R + 255) / 256, 256, 0, s>>>(off, sdist, R, cmin, cmax);
+  KNN_LAUNCH_CHECK();
+  return KNN_OK;
+}
+
+int launch_query_clusters(const uint64_t *skeys, const int32_t *off, int64_t m,
+                          int R, float *qrad, int32_t *slot_cl, cudaStream_t s) {
+  cluster_max_from_keys_kernel<<<(R + 255) / 256, 256, 0, s>>>(skeys, off, R, qrad);
+  KNN_LAUNCH_CHECK();
+  if (m > 0) {
+    slot_cluster_kernel<<<grid_for(m, 256), 256, 0, s>>>(skeys, m, slot_cl);
+    KNN_LAUNCH_CHECK();
+  }
+  return KNN_OK;
+}
+
+int launch_rep_dist(const float4 *qreps, int Rq, const float4 *sreps, int Rs,
+                    int dp4, float *drr, cudaStream_t s) {
+  rep_dist_kernel<<<grid_for((int64_t)Rq * Rs, 256), 256, 0, s>>>(qreps, Rq, sreps,
+                                                                 Rs, dp4, drr);
+  KNN_LAUNCH_CHECK();
+  return KNN_OK;
+}
+
+int launch_bounds_filter(const float *drr, int Rq, int Rs, const float *qrad,
+                         const int32_t *qoff, const int32_t *soff,
+                         const float *sdist, const float *scmax, int k, int d,
+                         float *theta0, int32_t *rlist, int32_t *rlen,
+                         cudaStream_t s) {
+  int p2 = 1;
+  while (p2 < Rs) p2 <<= 1;
+  size_t smem = (size_t)p2 * sizeof(uint64_t);
+  if (smem > 48 * 1024)
+    KNN_CUDA_TRY(cudaFuncSetAttribute(bounds_filter_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+  bounds_filter_kernel<<<Rq, 512, smem, s>>>(drr, Rq, Rs, qrad, qoff, soff, sdist,
+                                             scmax, k, d, p2, theta0, rlist, rlen);
+  KNN_LAUNCH_CHECK();
+  return KNN_OK;
+}
+
+}  // namespace knnsweet

@@ -1,0 +1,62 @@
+// kernels.cuh -- launcher declarations shared by the translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace knnsweet {
+
+// Arguments of the per-query scan.
+struct ScanArgs {
+  const float4 *qrows;      // m x dp4, original query order
+  const int32_t *qorder;    // slot -> query row (grouped by query cluster)
+  const int32_t *slot_cl;   // slot -> query cluster
+  int64_t m;
+  int d, dp4, dp4_tmpl, k;
+  const float4 *sreps;      // Rs x dp4 reference representatives
+  const float4 *srows;      // n x dp4, cluster-contiguous, ascending d(s,Rs)
+  const float *sdist;       // n: d(s, Rs) in the same order
+  const int32_t *sidx;      // n: original reference row
+  const int32_t *soff;      // Rs + 1 cluster offsets
+  const float *cmin, *cmax; // Rs: smallest / largest member distance
+  const float *theta0;      // Rq: initial k-th bound per query cluster
+  const int32_t *rlist;     // Rq x Rs surviving clusters, nearest first
+  const int32_t *rlen;      // Rq
+  int Rs;
+  int32_t *out_idx;         // m x k
+  float *out_dist;          // m x k
+  unsigned long long *work_counter;  // zeroed before launch
+  unsigned long long *counters;      // [evals, visited, pruned] or null
+};
+
+int launch_pack_rows(const float *src, int64_t n, int d, int dp4, float4 *dst,
+                     cudaStream_t s);
+int launch_rep_select(const float4 *rows, int dp4, const int32_t *cand_dev,
+                      int R, int trials, uint32_t *score_dev, float4 *reps,
+                      int32_t *rep_rows, cudaStream_t s);
+int launch_assign(const float4 *rows, int64_t n, int dp4, const float4 *reps,
+                  int R, int32_t *cl, float *dr, cudaStream_t s);
+size_t cluster_sort_temp_bytes(int64_t n, int R);
+int launch_cluster_sort(const int32_t *cl, const float *dr, int64_t n, int R,
+                        uint64_t *keys, int32_t *vals, uint64_t *skeys,
+                        int32_t *perm, void *temp, size_t temp_bytes,
+                        cudaStream_t s);
+int launch_cluster_layout(const uint64_t *skeys, const int32_t *perm, int64_t n,
+                          const float4 *rows, int dp4, float4 *srows,
+                          float *sdist, int32_t *sidx, cudaStream_t s);
+int launch_cluster_offsets(const uint64_t *skeys, int64_t n, int R, int32_t *off,
+                           cudaStream_t s);
+int launch_cluster_minmax(const int32_t *off, const float *sdist, int R,
+                          float *cmin, float *cmax, cudaStream_t s);
+int launch_query_clusters(const uint64_t *skeys, const int32_t *off, int64_t m,
+                          int R, float *qrad, int32_t *slot_cl, cudaStream_t s);
+int launch_rep_dist(const float4 *qreps, int Rq, const float4 *sreps, int Rs,
+                    int dp4, float *drr, cudaStream_t s);
+int launch_bounds_filter(const float *drr, int Rq, int Rs, const float *qrad,
+                         const int32_t *qoff, const int32_t *soff,
+                         const float *sdist, const float *scmax, int k, int d,
+                         float *theta0, int32_t *rlist, int32_t *rlen,
+                         cudaStream_t s);
+int launch_scan(const ScanArgs &a, int num_sms, cudaStream_t s);
+
+}  // namespace knnsweet

@@ -1,0 +1,118 @@
+"""CPU tests of the C ABI: the library loads, exports every function the
+header declares, its structs match the header's layout, and argument errors
+come back as status codes without touching a GPU."""
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from knn_sweet_b200 import _lib
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADERS = sorted((ROOT / "include").glob("*.h"))
+
+
+def declared_functions():
+    names = []
+    for h in HEADERS:
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"^[A-Za-z_][\w \*]*?\b(knn_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for want in ("knn_join", "knn_join_device", "knn_last_error", "knn_default_options"):
+        assert want in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(str(_lib.LIB_PATH))
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+        assert name in _lib.SIGNATURES, f"{name} has no ctypes signature"
+
+
+def test_struct_layout_matches_header(tmp_path):
+    src = tmp_path / "layout.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "knnsweet.h"\n'
+        "int main(void){\n"
+        'printf("%zu %zu %zu %zu %zu\\n", sizeof(knn_options), sizeof(knn_stats),'
+        " offsetof(knn_stats, ms_build), offsetof(knn_stats, qreps_used),"
+        " offsetof(knn_options, margin));\n"
+        "return 0;}\n")
+    exe = tmp_path / "layout"
+    cc = "/usr/bin/gcc" if Path("/usr/bin/gcc").exists() else "gcc"
+    subprocess.run([cc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    want = [ctypes.sizeof(_lib.KnnOptions), ctypes.sizeof(_lib.KnnStats),
+            _lib.KnnStats.ms_build.offset, _lib.KnnStats.qreps_used.offset,
+            _lib.KnnOptions.margin.offset]
+    assert [int(v) for v in out] == want
+
+
+def test_default_options():
+    o = _lib.default_options()
+    assert (o.qreps, o.sreps, o.seed, o.rep_trials, o.precision, o.margin, o.flags) == \
+        (0, 0, 2015, 10, _lib.KNN_FP32, 32, 0)
+    assert _lib.load().knn_abi_version() == 1
+
+
+def _call_join(q, r, d, k, opt=None, m=None, n=None):
+    lib = _lib.load()
+    m = q.shape[0] if m is None else m
+    n = r.shape[0] if n is None else n
+    idx = np.empty((max(m, 1), max(k, 1)), np.int32)
+    dist = np.empty((max(m, 1), max(k, 1)), np.float32)
+    return lib.knn_join(q.ctypes.data_as(ctypes.c_void_p), m, r.ctypes.data_as(ctypes.c_void_p), n,
+                        d, k, idx.ctypes.data_as(ctypes.c_void_p),
+                        dist.ctypes.data_as(ctypes.c_void_p),
+                        None if opt is None else ctypes.byref(opt), None)
+
+
+@pytest.mark.parametrize("d,k", [(0, 5), (-3, 5), (3, 0), (3, -1), (3, 1025)])
+def test_bad_sizes_are_rejected(d, k):
+    x = np.zeros((4, 3), np.float32)
+    assert _call_join(x, x, d, k) == _lib.KNN_EINVAL
+    assert _lib.load().knn_last_error()
+
+
+def test_bad_options_are_rejected():
+    x = np.zeros((4, 3), np.float32)
+    for field, val in [("flags", 1), ("qreps", -1), ("sreps", 9000), ("rep_trials", 0),
+                       ("precision", 7), ("margin", -2)]:
+        o = _lib.default_options()
+        setattr(o, field, val)
+        assert _call_join(x, x, 3, 2, opt=o) == _lib.KNN_EINVAL, field
+
+
+def test_empty_query_set_is_ok_without_gpu():
+    x = np.zeros((4, 3), np.float32)
+    assert _call_join(x, x, 3, 2, m=0) == _lib.KNN_OK
+
+
+def test_null_pointers_rejected():
+    lib = _lib.load()
+    out = np.empty((4, 2), np.int32)
+    rc = lib.knn_join(None, 4, None, 4, 3, 2, out.ctypes.data_as(ctypes.c_void_p),
+                      out.ctypes.data_as(ctypes.c_void_p), None, None)
+    assert rc == _lib.KNN_EINVAL
+    rc = lib.knn_backward_device(None, 4, None, 4, 3, 2, None, None, None, None, None)
+    assert rc == _lib.KNN_EINVAL
+    rc = lib.knn_backward_device(None, 4, None, 4, 0, 2, None, None, None, None, None)
+    assert rc == _lib.KNN_EINVAL
+
+
+def test_pack_indexdist_layout():
+    from knn_sweet_b200 import pack_indexdist
+    idx = np.array([[3, 1], [0, -1]], np.int32)
+    dist = np.array([[0.5, 2.0], [0.0, np.inf]], np.float32)
+    rec = pack_indexdist(idx, dist)
+    raw = rec.view(np.int32).reshape(-1)
+    assert raw[0] == 3 and raw[2] == 1 and raw[4] == 0 and raw[6] == -1
+    assert rec["dist"][0, 1] == 2.0 and np.isinf(rec["dist"][1, 1])

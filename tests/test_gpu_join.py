@@ -1,0 +1,152 @@
+"""GPU parity tests of the plain FP32 pruned join against the FP64 oracle.
+
+Bar: identical neighbour index lists under the (distance, lower index) order;
+FP32 distances within 1e-5 relative of the FP64 oracle (bit-exact on integer
+data, where every FP32 squared distance is an exact integer).  On float data
+an index may differ from the oracle only where the oracle's own distances
+tie within 1e-5 relative (FP32 rounding can order such a pair either way).
+"""
+import numpy as np
+import pytest
+
+from knn_sweet_b200 import data, knnjoin
+from tests.golden.make_golden import load_cases
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-5
+
+
+def assert_matches(idx, dist, oi, od, exact: bool):
+    idx = np.asarray(idx)
+    dist = np.asarray(dist)
+    if exact:
+        assert np.array_equal(idx, oi)
+        assert np.array_equal(dist, od.astype(np.float32))
+        return
+    fin = np.isfinite(od)
+    assert np.array_equal(np.isfinite(dist), fin)
+    np.testing.assert_allclose(dist[fin], od[fin], rtol=REL, atol=0)
+    bad = np.argwhere(idx != oi)
+    for i, j in bad:
+        # only a near-tie in the oracle may swap
+        v = od[i, j]
+        near = np.abs(od[i] - v) <= REL * max(v, 1e-30)
+        assert near.sum() >= 2, (i, j, idx[i, j], oi[i, j])
+
+
+def torch_join(q, r, k, **kw):
+    import torch
+    qt = torch.from_numpy(q).cuda()
+    rt = qt if r is q else torch.from_numpy(r).cuda()
+    out = knnjoin(qt, None if r is q else rt, k, **kw)
+    torch.cuda.synchronize()
+    return tuple(o.cpu().numpy() if hasattr(o, "cpu") else o for o in out)
+
+
+@pytest.mark.parametrize("name", sorted(load_cases()))
+def test_golden_cases_device_path(cuda_device, name):
+    q, r, k, oi, od = load_cases()[name]
+    same = np.array_equal(q, r)
+    idx, dist = torch_join(q, q if same else r, k)
+    exact = bool(np.all(q == np.rint(q)) and np.all(r == np.rint(r)))
+    assert_matches(idx, dist, oi, od, exact)
+
+
+@pytest.mark.parametrize("name", sorted(load_cases()))
+def test_golden_cases_host_path(cuda_device, name):
+    q, r, k, oi, od = load_cases()[name]
+    idx, dist = knnjoin(q, r, k)
+    exact = bool(np.all(q == np.rint(q)) and np.all(r == np.rint(r)))
+    assert_matches(idx, dist, oi, od, exact)
+
+
+@pytest.mark.parametrize("k", [1, 16, 100, 200, 256, 257, 600, 1000])
+def test_skin_like_selfjoin_k(cuda_device, oracle, k):
+    x = data.skin_like(30000, seed=21)
+    rows = np.random.default_rng(k).choice(30000, 300, replace=False)
+    idx, dist, st = knnjoin(x, None, k, qreps=120, sreps=120, stats=True)
+    oi, od = oracle.bruteforce_f64(x, x, k, qrows=rows)
+    assert_matches(idx[rows], dist[rows], oi, od, exact=True)
+    assert 0 < st.dist_evals <= st.pairs_total
+    assert st.pairs_pruned == st.pairs_total - st.dist_evals
+    assert np.all(np.diff(dist, axis=1) >= 0)
+
+
+@pytest.mark.parametrize("d,k", [(1, 5), (2, 9), (5, 7), (8, 32), (16, 64), (32, 32),
+                                 (33, 10), (64, 100), (128, 100)])
+def test_float_dims(cuda_device, oracle, d, k):
+    r, q = data.gaussian_mix(20000, 1000, d, 40, seed=100 + d)
+    idx, dist = knnjoin(q, r, k)
+    oi, od = oracle.bruteforce_f64(q, r, k)
+    assert_matches(idx, dist, oi, od, exact=False)
+
+
+def test_cross_join_separate_reps(cuda_device, oracle):
+    r = data.skin_like(25000, seed=31)
+    q = data.skin_like(4000, seed=32)
+    idx, dist = knnjoin(q, r, 50, qreps=40, sreps=200)
+    oi, od = oracle.bruteforce_f64(q, r, 50)
+    assert_matches(idx, dist, oi, od, exact=True)
+
+
+def test_edge_sizes(cuda_device, oracle):
+    rng = np.random.default_rng(7)
+    for m, n, k in [(1, 1, 1), (1, 5, 8), (7, 3, 4), (3, 300, 300), (50, 50, 50)]:
+        q = rng.integers(0, 4, size=(m, 3)).astype(np.float32)
+        r = rng.integers(0, 4, size=(n, 3)).astype(np.float32)
+        idx, dist = knnjoin(q, r, k)
+        oi, od = oracle.bruteforce_f64(q, r, k)
+        assert_matches(idx, dist, oi, od, exact=True)
+
+
+def test_empty_reference_set(cuda_device):
+    q = np.ones((4, 3), np.float32)
+    r = np.zeros((0, 3), np.float32)
+    idx, dist = knnjoin(q, r, 3)
+    assert (idx == -1).all() and np.isinf(dist).all()
+
+
+def test_all_identical_points(cuda_device):
+    x = np.full((5000, 3), 7.0, np.float32)
+    idx, dist = knnjoin(x, None, 64)
+    assert (dist == 0).all()
+    assert (idx == np.arange(64)[None, :]).all()
+
+
+def test_deterministic_and_apis_agree(cuda_device):
+    x = data.skin_like(20000, seed=41)
+    a = knnjoin(x, None, 100)
+    b = knnjoin(x, None, 100)
+    c = torch_join(x, x, 100)
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v)
+    for u, v in zip(a, c):
+        assert np.array_equal(u, v)
+
+
+def test_rep_counts_do_not_change_result(cuda_device):
+    x = data.skin_like(15000, seed=51)
+    base = knnjoin(x, None, 32, qreps=1, sreps=1)
+    for reps in (7, 64, 500, 4096):
+        got = knnjoin(x, None, 32, qreps=reps, sreps=reps)
+        assert np.array_equal(base[0], got[0]) and np.array_equal(base[1], got[1])
+
+
+def test_full_size_skin_selfjoin_properties(cuda_device, oracle):
+    """The full self-join workload (245,057 points, k=200, 800/800 reps):
+    size-independent properties on all rows, oracle comparison on a sample."""
+    x = data.skin_like(seed=1)
+    idx, dist, st = knnjoin(x, None, 200, qreps=800, sreps=800, stats=True)
+    n = x.shape[0]
+    assert idx.shape == (n, 200)
+    assert np.all(np.diff(dist, axis=1) >= 0)
+    assert (idx >= 0).all() and (idx < n).all()
+    assert (dist[:, 0] == 0).all()
+    # no duplicate neighbour in a row
+    s = np.sort(idx, axis=1)
+    assert not np.any(s[:, 1:] == s[:, :-1])
+    rows = np.random.default_rng(3).choice(n, 256, replace=False)
+    oi, od = oracle.bruteforce_f64(x, x, 200, qrows=rows)
+    assert_matches(idx[rows], dist[rows], oi, od, exact=True)
+    assert st.dist_evals < 0.05 * st.pairs_total
