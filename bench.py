@@ -147,20 +147,26 @@ class ClockSampler:
 # CPU baseline: the reference's pruned method restated on the host (oracle)
 # ----------------------------------------------------------------------------
 def cpu_port_time(x: np.ndarray, sample: int, threads: int, seed: int = 7):
-    """Seconds for the full-size join estimated from a bounded sample:
-    index build on the full set + scan of `sample` queries scaled to all."""
+    """Seconds for the full-size join estimated from a bounded sample: the
+    port's own timers give the index build on the full set and the scan of
+    `sample` random queries; the scan is scaled to all queries."""
     from oracle import oracle as orc
     m = x.shape[0]
+    sample = min(sample, m)
     rows = np.random.default_rng(seed).choice(m, sample, replace=False).astype(np.int64)
-    t0 = time.perf_counter()
-    orc.port_join(x, x, K, REPS, REPS, qrows=rows[:1], threads=threads)
-    t_build = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    orc.port_join(x, x, K, REPS, REPS, qrows=rows, threads=threads)
-    t_all = time.perf_counter() - t0
-    t_scan = max(t_all - t_build, 1e-9)
+    _, _, st = orc.port_join(x, x, K, REPS, REPS, qrows=rows, threads=threads)
+    t_build, t_scan = st["build_seconds"], max(st["scan_seconds"], 1e-9)
     est = t_build + t_scan * m / sample
     return est, t_build, t_scan
+
+
+def cpu_sample_size(x: np.ndarray, threads: int, scan_budget_s: float) -> int:
+    """Queries whose scan takes about scan_budget_s on the host (pilot run)."""
+    m = x.shape[0]
+    pilot = min(m, 2000)
+    _, _, ts = cpu_port_time(x, pilot, threads, seed=1)
+    per_query = ts / pilot
+    return int(max(pilot, min(m, scan_budget_s / max(per_query, 1e-9))))
 
 
 def run_reference(args):
@@ -171,7 +177,10 @@ def run_reference(args):
     x = data.skin_like(args.n, seed=1)
     m = x.shape[0]
     cores = host_cores()
-    sample = max(64, m // 200)
+    # each step: full index build + a query sample, sized so that the whole
+    # run stays within about three minutes
+    budget = max(0.2, 150.0 / (args.warmup + args.steps) - 0.7)
+    sample = cpu_sample_size(x, cores, budget)
     times = []
     for it in range(args.warmup + args.steps):
         est, tb, ts = cpu_port_time(x, sample, cores, seed=100 + it)
@@ -332,7 +341,7 @@ def run_ours(args):
         line["e2e"] = e2e
     if world == 1 and not args.no_cpu_baseline:
         cores = host_cores()
-        sample = max(64, m // 100)
+        sample = cpu_sample_size(x, cores, 10.0)
         est, tb, ts = cpu_port_time(x, sample, cores)
         line["cpu_baseline"] = {
             "value": m / est, "unit": "queries/s", "cores": cores, "kind": "port",

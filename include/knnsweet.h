@@ -81,6 +81,8 @@ typedef struct knn_stats {
   int64_t clusters_visited; /* (query, reference cluster) pairs scanned        */
   int64_t clusters_pruned;  /* (query, reference cluster) pairs skipped whole  */
   int64_t refine_rechecks;  /* BF16 form: candidates re-checked in FP64        */
+  int64_t topk_candidates;  /* candidates that beat the running k-th key       */
+  int64_t topk_merges;      /* sorted merges of candidate buffers into top-k   */
   float ms_build;           /* representative sampling .. cluster filter      */
   float ms_search;          /* per-query pruned scan                          */
   float ms_total;           /* whole call, device time                        */
@@ -136,6 +138,14 @@ int knn_backward_device(const float *q, int64_t m, const float *r, int64_t n,
                         int32_t d, int32_t k, const int32_t *idx,
                         const float *grad_dist2, float *grad_q, float *grad_r,
                         void *stream);
+
+/*
+ * Returns the device scratch memory the library keeps cached between calls
+ * (one stream-ordered pool per device; no reference counterpart: the
+ * reference never frees its device memory).  Memory still in use by calls in
+ * flight is kept.
+ */
+int knn_trim_memory(void);
 
 /*
  * Interleave SoA results into the reference's IndexDist layout

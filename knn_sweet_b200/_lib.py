@@ -47,6 +47,8 @@ class KnnStats(ctypes.Structure):
         ("clusters_visited", ctypes.c_int64),
         ("clusters_pruned", ctypes.c_int64),
         ("refine_rechecks", ctypes.c_int64),
+        ("topk_candidates", ctypes.c_int64),
+        ("topk_merges", ctypes.c_int64),
         ("ms_build", ctypes.c_float),
         ("ms_search", ctypes.c_float),
         ("ms_total", ctypes.c_float),
@@ -71,6 +73,7 @@ SIGNATURES = {
     "knn_backward_device": (_c_int, [_vp, _c_i64, _vp, _c_i64, _c_i32, _c_i32, _vp, _vp,
                                      _vp, _vp, _vp]),
     "knn_pack_indexdist": (None, [_vp, _vp, _c_i64, _vp]),
+    "knn_trim_memory": (_c_int, []),
 }
 
 _lock = threading.Lock()

@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -46,6 +47,38 @@ void set_error(const char *fmt, ...) {
 
 namespace {
 
+// One stream-ordered memory pool per device for the library's scratch.  Its
+// release threshold is unlimited, so memory freed at the end of a call stays
+// cached for the next call instead of going back to the driver at every
+// synchronisation (knn_trim_memory() returns it).
+constexpr int kMaxDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[kMaxDevices] = {};
+
+int scratch_pool(cudaMemPool_t *out) {
+  int dev = 0;
+  KNN_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("device ordinal %d out of range", dev);
+    return KNN_EINVAL;
+  }
+  std::lock_guard<std::mutex> guard(g_pool_mu);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool;
+    KNN_CUDA_TRY(cudaMemPoolCreate(&pool, &props));
+    uint64_t threshold = UINT64_MAX;
+    KNN_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    g_pools[dev] = pool;
+  }
+  *out = g_pools[dev];
+  return KNN_OK;
+}
+
 // Stream-ordered scratch: every allocation is released on the same stream
 // when the arena goes out of scope.
 class Arena {
@@ -61,8 +94,12 @@ class Arena {
   int alloc(T **out, size_t count) {
     *out = nullptr;
     if (count == 0) count = 1;
+    if (!pool_) {
+      int rc = scratch_pool(&pool_);
+      if (rc != KNN_OK) return rc;
+    }
     void *p = nullptr;
-    cudaError_t e = cudaMallocAsync(&p, count * sizeof(T), s_);
+    cudaError_t e = cudaMallocFromPoolAsync(&p, count * sizeof(T), pool_, s_);
     if (e != cudaSuccess) {
       cudaGetLastError();
       set_error("device allocation of %zu bytes failed: %s", count * sizeof(T),
@@ -76,6 +113,7 @@ class Arena {
 
  private:
   cudaStream_t s_;
+  cudaMemPool_t pool_ = nullptr;
   std::vector<void *> ptrs_;
 };
 
@@ -247,7 +285,7 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
   if (st) memset(st, 0, sizeof *st);
   launch_counter() = 0;
   if (m == 0) return KNN_OK;
-  if (!q || !r || !out_idx || !out_dist) {
+  if (!q || (!r && n > 0) || !out_idx || !out_dist) {
     set_error("null pointer argument");
     return KNN_EINVAL;
   }
@@ -304,8 +342,10 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
   KNN_TRY(ar.alloc(&sidx, (size_t)n));
   KNN_TRY(ar.alloc(&cmin, (size_t)Rs));
   KNN_TRY(ar.alloc(&cmax, (size_t)Rs));
-  KNN_TRY(launch_cluster_layout(sset.skeys, sset.perm, n, Rp, dp4s, srows, sdist,
-                                sidx, s));
+  // rows with a spare pad float carry their index there (register-width rows)
+  const bool idx_in_row = tmpl > 0 && 4 * dp4s > d;
+  KNN_TRY(launch_cluster_layout(sset.skeys, sset.perm, n, Rp, dp4s, idx_in_row, srows,
+                                sdist, sidx, s));
   KNN_TRY(launch_cluster_minmax(sset.off, sdist, Rs, cmin, cmax, s));
 
   if (share) {
@@ -330,8 +370,8 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
   KNN_TRY(evs.record(1, s));
 
   unsigned long long *ctr;
-  KNN_TRY(ar.alloc(&ctr, 4));
-  KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, 4 * sizeof(unsigned long long), s));
+  KNN_TRY(ar.alloc(&ctr, 6));
+  KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, 6 * sizeof(unsigned long long), s));
   ScanArgs a{};
   a.qrows = Qp;
   a.qorder = qset.perm;
@@ -341,6 +381,7 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
   a.dp4 = dp4s;
   a.dp4_tmpl = tmpl;
   a.k = k;
+  a.idx_in_row = idx_in_row;
   a.sreps = sset.reps;
   a.srows = srows;
   a.sdist = sdist;
@@ -360,12 +401,14 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
   KNN_TRY(evs.record(2, s));
 
   if (st) {
-    unsigned long long h[4];
+    unsigned long long h[6];
     KNN_CUDA_TRY(cudaMemcpyAsync(h, ctr, sizeof h, cudaMemcpyDeviceToHost, s));
     KNN_CUDA_TRY(cudaStreamSynchronize(s));
     st->dist_evals = (int64_t)h[1];
     st->clusters_visited = (int64_t)h[2];
     st->clusters_pruned = (int64_t)h[3];
+    st->topk_candidates = (int64_t)h[4];
+    st->topk_merges = (int64_t)h[5];
     st->pairs_pruned = st->pairs_total - st->dist_evals;
     st->qreps_used = Rq;
     st->sreps_used = Rs;
@@ -471,6 +514,20 @@ int knn_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d,
   }
   cudaStreamDestroy(s);
   return rc;
+}
+
+int knn_trim_memory(void) {
+  error_buffer().clear();
+  std::lock_guard<std::mutex> guard(g_pool_mu);
+  for (int d = 0; d < kMaxDevices; d++) {
+    if (!g_pools[d]) continue;
+    cudaError_t e = cudaMemPoolTrimTo(g_pools[d], 0);
+    if (e != cudaSuccess) {
+      set_error("cudaMemPoolTrimTo failed: %s", cudaGetErrorString(e));
+      return KNN_ECUDA;
+    }
+  }
+  return KNN_OK;
 }
 
 void knn_pack_indexdist(const int32_t *idx, const float *dist, int64_t count,

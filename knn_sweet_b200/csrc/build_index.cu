@@ -186,11 +186,14 @@ __global__ void cluster_keys_kernel(const int32_t *__restrict__ cl,
 // Cluster-contiguous layout: row p of the sorted set is input row perm[p];
 // its distance to the representative is the low word of its key.
 // (fillTMembers + host sort, knnjoin.cu:106-113, 382-399, without the
-// per-cluster device<->host round trips.)
+// per-cluster device<->host round trips.)  With idx_in_row the last pad float
+// of every row carries the original row index, so the scan gets coordinates
+// and index from one load.
 __global__ void cluster_layout_kernel(const uint64_t *__restrict__ skeys,
                                       const int32_t *__restrict__ perm,
                                       int64_t n, const float4 *__restrict__ rows,
-                                      int dp4, float4 *__restrict__ srows,
+                                      int dp4, bool idx_in_row,
+                                      float4 *__restrict__ srows,
                                       float *__restrict__ sdist,
                                       int32_t *__restrict__ sidx) {
   int64_t total = n * dp4;
@@ -199,7 +202,9 @@ __global__ void cluster_layout_kernel(const uint64_t *__restrict__ skeys,
     int64_t p = t / dp4;
     int c = (int)(t - p * dp4);
     int32_t src = perm[p];
-    srows[t] = rows[(int64_t)src * dp4 + c];
+    float4 v = rows[(int64_t)src * dp4 + c];
+    if (idx_in_row && c == dp4 - 1) v.w = __int_as_float(src);
+    srows[t] = v;
     if (c == 0) {
       if (sdist) sdist[p] = __uint_as_float((uint32_t)(skeys[p] & 0xffffffffu));
       if (sidx) sidx[p] = src;
@@ -489,11 +494,12 @@ int launch_cluster_sort(const int32_t *cl, const float *dr, int64_t n, int R,
 }
 
 int launch_cluster_layout(const uint64_t *skeys, const int32_t *perm, int64_t n,
-                          const float4 *rows, int dp4, float4 *srows,
-                          float *sdist, int32_t *sidx, cudaStream_t s) {
+                          const float4 *rows, int dp4, bool idx_in_row,
+                          float4 *srows, float *sdist, int32_t *sidx,
+                          cudaStream_t s) {
   if (n == 0) return KNN_OK;
   cluster_layout_kernel<<<grid_for(n * dp4, 256), 256, 0, s>>>(
-      skeys, perm, n, rows, dp4, srows, sdist, sidx);
+      skeys, perm, n, rows, dp4, idx_in_row, srows, sdist, sidx);
   KNN_LAUNCH_CHECK();
   return KNN_OK;
 }

@@ -13,6 +13,7 @@ struct ScanArgs {
   const int32_t *slot_cl;   // slot -> query cluster
   int64_t m;
   int d, dp4, dp4_tmpl, k;
+  bool idx_in_row;          // srows carry the index in their last pad float
   const float4 *sreps;      // Rs x dp4 reference representatives
   const float4 *srows;      // n x dp4, cluster-contiguous, ascending d(s,Rs)
   const float *sdist;       // n: d(s, Rs) in the same order
@@ -26,7 +27,7 @@ struct ScanArgs {
   int32_t *out_idx;         // m x k
   float *out_dist;          // m x k
   unsigned long long *work_counter;  // zeroed before launch
-  unsigned long long *counters;      // [evals, visited, pruned] or null
+  unsigned long long *counters;      // [evals, visited, pruned, pushed, merges]
 };
 
 int launch_pack_rows(const float *src, int64_t n, int d, int dp4, float4 *dst,
@@ -42,8 +43,9 @@ int launch_cluster_sort(const int32_t *cl, const float *dr, int64_t n, int R,
                         int32_t *perm, void *temp, size_t temp_bytes,
                         cudaStream_t s);
 int launch_cluster_layout(const uint64_t *skeys, const int32_t *perm, int64_t n,
-                          const float4 *rows, int dp4, float4 *srows,
-                          float *sdist, int32_t *sidx, cudaStream_t s);
+                          const float4 *rows, int dp4, bool idx_in_row,
+                          float4 *srows, float *sdist, int32_t *sidx,
+                          cudaStream_t s);
 int launch_cluster_offsets(const uint64_t *skeys, int64_t n, int R, int32_t *off,
                            cudaStream_t s);
 int launch_cluster_minmax(const int32_t *off, const float *sdist, int R,

@@ -5,46 +5,212 @@
 // One warp per query, persistent blocks pulling query slots from an atomic
 // counter in query-cluster order (the reference's reorder_members,
 // knnjoin.cu:114-124, 768), so neighbouring warps walk the same candidate
-// list.  For every surviving reference cluster Rs of the query's cluster
-// (nearest representative first):
-//   - 32 clusters at a time, each lane computes D = d(q, Rs) and drops the
-//     cluster if  D - radius(Rs) > theta  or  D + theta < min member
-//     distance: no member can be within theta (the reference's first-member
-//     `break`, knnjoin.cu:797).
-//   - Members are stored contiguously, ascending by d(s, Rs).  The members
-//     that can be within theta of q satisfy |D - d(s,Rs)| <= theta
-//     (knnjoin.cu:796-801), a contiguous band: its lower end is found by a
-//     warp-wide 32-ary search, and the warp walks the band 32 members per
-//     step with coalesced float4 row loads, stopping as soon as a whole step
-//     lies above D + theta.
-//   - Exact FP32 distances of band members go through the warp top-k:
-//     candidates whose (d^2, index) key beats the current k-th key are
-//     appended to a shared-memory buffer; a full buffer is bitonic-sorted and
-//     merged into the sorted list of the k best, and theta drops to the new
-//     k-th distance.  This replaces the per-thread insertion sort into an
-//     8 KB local-memory array (knnjoin.cu:774, 813-845).
+// list.  For the surviving reference clusters Rs of the query's cluster,
+// 32 at a time:
+//   - each lane computes D = d(q, Rs) and drops its cluster if
+//     D - radius(Rs) > theta or D + theta < smallest member distance: no
+//     member can be within theta (the reference's first-member `break`,
+//     knnjoin.cu:797); the survivors are visited nearest first (a warp sort
+//     on D), so the running k-th distance theta falls early.
+//   - Members are stored contiguously, ascending by d(s, Rs).  Members within
+//     theta of q satisfy |D - d(s,Rs)| <= theta (knnjoin.cu:796-801), a
+//     contiguous band around the member whose d(s,Rs) is closest to D.  A
+//     warp-wide 32-ary search finds that member; the warp then walks outward,
+//     32 members per step, alternately up and down, with coalesced row loads,
+//     and stops in each direction at the first step that leaves the band
+//     (re-evaluated with the current theta).
+//   - Exact FP32 distances go through the warp top-k: candidates whose
+//     (d^2, index) key beats the current k-th key are appended to a
+//     shared-memory buffer; a full buffer is sorted and merged into the sorted
+//     list of the k best, after which theta is the new k-th distance.  For
+//     k <= 256 the list lives in registers (8 keys per lane at most) and the
+//     sort/merge runs on warp shuffles; above 256 both live in shared memory.
+//     This replaces the per-thread insertion into an 8 KB local-memory array
+//     (knnjoin.cu:774, 813-845).
 // Bounds are widened by a rounding slack (bound_tol) so that FP32 rounding
 // never prunes a point that the FP32 distances would rank in the top k.
+#include <type_traits>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
 namespace knnsweet {
 
+__device__ __forceinline__ uint64_t shfl_xor64(uint64_t v, int m) {
+  uint32_t lo = __shfl_xor_sync(kFull, (uint32_t)v, m);
+  uint32_t hi = __shfl_xor_sync(kFull, (uint32_t)(v >> 32), m);
+  return ((uint64_t)hi << 32) | lo;
+}
+__device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) {
+  uint32_t lo = __shfl_sync(kFull, (uint32_t)v, src);
+  uint32_t hi = __shfl_sync(kFull, (uint32_t)(v >> 32), src);
+  return ((uint64_t)hi << 32) | lo;
+}
+__device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+__device__ __forceinline__ uint64_t umax64(uint64_t a, uint64_t b) { return a < b ? b : a; }
+
+// ---------------------------------------------------------------------------
+// Register bitonic networks over 32*E keys, blocked layout: lane l holds
+// positions E*l .. E*l+E-1.  Strides >= E pair registers of different lanes
+// (shuffle), smaller strides pair registers of the same lane.
+// ---------------------------------------------------------------------------
+// Only the within-lane strides are unrolled (their register indices must be
+// static); the cross-lane strides run as a loop, which keeps the live range
+// of the network, and so the register count, small.
+template <int E>
+__device__ __forceinline__ void reg_cross_step(uint64_t (&x)[E], int lane, int size,
+                                               int stride) {
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    const int i = E * lane + j;
+    const bool up = (i & size) == 0;
+    const bool lower = (i & stride) == 0;
+    const uint64_t o = shfl_xor64(x[j], stride / E);
+    x[j] = (lower == up) ? umin64(x[j], o) : umax64(x[j], o);
+  }
+}
+
+template <int E>
+__device__ __forceinline__ void reg_inner_steps(uint64_t (&x)[E], int lane, int size) {
+#pragma unroll
+  for (int stride = E / 2; stride > 0; stride >>= 1) {
+    if (stride < size) {
+#pragma unroll
+      for (int j = 0; j < E; j++) {
+        if ((j & stride) == 0) {
+          const int j2 = j | stride;
+          const bool up = ((E * lane + j) & size) == 0;
+          const uint64_t a = x[j], b = x[j2];
+          const bool sw = (a > b) == up;
+          x[j] = sw ? b : a;
+          x[j2] = sw ? a : b;
+        }
+      }
+    }
+  }
+}
+
+template <int E>
+__device__ __forceinline__ void reg_bitonic_sort(uint64_t (&x)[E], int lane) {
+  constexpr int L = 32 * E;
+#pragma unroll 1
+  for (int size = 2; size <= L; size <<= 1) {
+#pragma unroll 1
+    for (int stride = size >> 1; stride >= E; stride >>= 1)
+      reg_cross_step<E>(x, lane, size, stride);
+    reg_inner_steps<E>(x, lane, size);
+  }
+}
+
+// Sorts a bitonic sequence ascending (every comparison ascending: size = 2L).
+template <int E>
+__device__ __forceinline__ void reg_bitonic_merge(uint64_t (&x)[E], int lane) {
+  constexpr int L = 32 * E;
+#pragma unroll 1
+  for (int stride = L >> 1; stride >= E; stride >>= 1)
+    reg_cross_step<E>(x, lane, 2 * L, stride);
+  reg_inner_steps<E>(x, lane, 2 * L);
+}
+
+// Shared part of both top-k variants: the append buffer and the threshold.
+struct TopKBase {
+  uint64_t *buf;  // append buffer (shared memory)
+  int nbuf, nlist, k;
+  uint64_t thr;   // a candidate enters iff its key < thr
+  float theta;    // distance matching thr (bound for the pruning tests)
+  unsigned pushed = 0, merges = 0;  // statistics of the current query (warp-uniform)
+
+  __device__ __forceinline__ void reset_threshold(float th0) {
+    nbuf = 0;
+    nlist = 0;
+    theta = th0;
+    // admits every d^2 <= th0^2, whatever the index
+    thr = ((uint64_t)__float_as_uint(th0 * th0) << 32) | 0xffffffffull;
+  }
+};
+
+// k <= 256: the sorted list of the best keys lives in registers.
+template <int E>
+struct RegTopK : TopKBase {
+  static constexpr int L = 32 * E;
+  static constexpr int kCap = L;       // candidate buffer capacity
+  static constexpr int kSmemKeys = L;  // per warp
+  uint64_t v[E];
+
+  __device__ __forceinline__ int cap() const { return kCap; }
+
+  __device__ __forceinline__ void init(uint64_t *wsm) { buf = wsm; }
+
+  __device__ __forceinline__ void reset(float th0, int) {
+#pragma unroll
+    for (int j = 0; j < E; j++) v[j] = kKeyMax;
+    reset_threshold(th0);
+  }
+
+  __device__ __forceinline__ void flush(int lane) {
+    if (nbuf == 0) return;
+    __syncwarp();
+    uint64_t b[E];
+#pragma unroll
+    for (int j = 0; j < E; j++) {
+      const int p = j * 32 + lane;  // any order: the buffer gets sorted
+      b[j] = p < nbuf ? buf[p] : kKeyMax;
+    }
+    __syncwarp();
+    reg_bitonic_sort<E>(b, lane);
+    // v ascending, b ascending: min(v[i], b[L-1-i]) holds the L smallest of
+    // both as a bitonic sequence.
+#pragma unroll
+    for (int j = 0; j < E; j++) v[j] = umin64(v[j], shfl64(b[E - 1 - j], 31 - lane));
+    reg_bitonic_merge<E>(v, lane);
+    nlist = min(k, nlist + nbuf);
+    merges++;
+    nbuf = 0;
+#pragma unroll
+    for (int j = 0; j < E; j++)
+      if (E * lane + j >= k) v[j] = kKeyMax;
+    if (nlist == k) {
+      const int kl = (k - 1) / E, kj = (k - 1) % E;
+      uint64_t mine = kKeyMax;
+#pragma unroll
+      for (int j = 0; j < E; j++)
+        if (j == kj) mine = v[j];
+      thr = shfl64(mine, kl);
+      theta = sqrtf(key_d2(thr));
+    }
+  }
+
+  // Writes the k results (through the buffer for coalesced stores).
+  __device__ __forceinline__ void write_out(int32_t *oi, float *od, int lane) {
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < E; j++) buf[E * lane + j] = v[j];
+    __syncwarp();
+    for (int t = lane; t < k; t += 32) {
+      const uint64_t key = buf[t];
+      const bool none = key == kKeyMax;
+      oi[t] = none ? -1 : key_idx(key);
+      od[t] = none ? __int_as_float(0x7f800000) : sqrtf(key_d2(key));
+    }
+    __syncwarp();
+  }
+};
+
 // Bitonic sort of L keys in shared memory, ascending, by one warp.
 template <int L>
-__device__ __forceinline__ void warp_bitonic_sort(uint64_t *s, int lane) {
+__device__ __forceinline__ void smem_bitonic_sort(uint64_t *s, int lane) {
 #pragma unroll 1
   for (int size = 2; size <= L; size <<= 1) {
 #pragma unroll 1
     for (int stride = size >> 1; stride > 0; stride >>= 1) {
 #pragma unroll
       for (int t0 = 0; t0 < (L / 2 + 31) / 32; t0++) {
-        int t = t0 * 32 + lane;
+        const int t = t0 * 32 + lane;
         if (t < L / 2) {
-          int i = 2 * t - (t & (stride - 1));
-          int j = i + stride;
-          bool up = (i & size) == 0;
-          uint64_t a = s[i], b = s[j];
+          const int i = 2 * t - (t & (stride - 1));
+          const int j = i + stride;
+          const bool up = (i & size) == 0;
+          const uint64_t a = s[i], b = s[j];
           if ((a > b) == up) {
             s[i] = b;
             s[j] = a;
@@ -56,18 +222,17 @@ __device__ __forceinline__ void warp_bitonic_sort(uint64_t *s, int lane) {
   }
 }
 
-// Sorts a bitonic sequence of L keys ascending (half-cleaner cascade).
 template <int L>
-__device__ __forceinline__ void warp_bitonic_merge(uint64_t *s, int lane) {
+__device__ __forceinline__ void smem_bitonic_merge(uint64_t *s, int lane) {
 #pragma unroll 1
   for (int stride = L >> 1; stride > 0; stride >>= 1) {
 #pragma unroll
     for (int t0 = 0; t0 < (L / 2 + 31) / 32; t0++) {
-      int t = t0 * 32 + lane;
+      const int t = t0 * 32 + lane;
       if (t < L / 2) {
-        int i = 2 * t - (t & (stride - 1));
-        int j = i + stride;
-        uint64_t a = s[i], b = s[j];
+        const int i = 2 * t - (t & (stride - 1));
+        const int j = i + stride;
+        const uint64_t a = s[i], b = s[j];
         if (a > b) {
           s[i] = b;
           s[j] = a;
@@ -78,26 +243,25 @@ __device__ __forceinline__ void warp_bitonic_merge(uint64_t *s, int lane) {
   }
 }
 
-// Warp-wide top-k state: `list` holds the nlist best keys (ascending, the
-// rest kKeyMax), `buf` the nbuf not yet merged candidates, `thr` the key a
-// candidate must beat and `theta` the matching distance.
-template <int L>
-struct WarpTopK {
+// k > 256: list and buffer both in shared memory.
+template <int LL>
+struct SmemTopK : TopKBase {
+  static constexpr int L = LL;
+  static constexpr int kCap = L;
+  static constexpr int kSmemKeys = 2 * L;
   uint64_t *list;
-  uint64_t *buf;
-  int nlist, nbuf, k;
-  uint64_t thr, thr0;
-  float theta, theta0;
+
+  __device__ __forceinline__ int cap() const { return kCap; }
+
+  __device__ __forceinline__ void init(uint64_t *wsm) {
+    list = wsm;
+    buf = wsm + L;
+  }
 
   __device__ __forceinline__ void reset(float th0, int lane) {
+    __syncwarp();
     for (int i = lane; i < L; i += 32) list[i] = kKeyMax;
-    nlist = 0;
-    nbuf = 0;
-    theta0 = th0;
-    theta = th0;
-    // admits every d^2 <= th0^2, whatever the index
-    thr0 = ((uint64_t)__float_as_uint(th0 * th0) << 32) | 0xffffffffull;
-    thr = thr0;
+    reset_threshold(th0);
     __syncwarp();
   }
 
@@ -106,14 +270,12 @@ struct WarpTopK {
     __syncwarp();
     for (int i = nbuf + lane; i < L; i += 32) buf[i] = kKeyMax;
     __syncwarp();
-    warp_bitonic_sort<L>(buf, lane);
-    for (int i = lane; i < L; i += 32) {
-      uint64_t a = list[i], b = buf[L - 1 - i];
-      list[i] = a < b ? a : b;
-    }
+    smem_bitonic_sort<L>(buf, lane);
+    for (int i = lane; i < L; i += 32) list[i] = umin64(list[i], buf[L - 1 - i]);
     __syncwarp();
-    warp_bitonic_merge<L>(list, lane);
+    smem_bitonic_merge<L>(list, lane);
     nlist = min(k, nlist + nbuf);
+    merges++;
     nbuf = 0;
     for (int i = k + lane; i < L; i += 32) list[i] = kKeyMax;
     __syncwarp();
@@ -123,43 +285,217 @@ struct WarpTopK {
     }
   }
 
-  // Offer one key per lane (kKeyMax = nothing).
-  __device__ __forceinline__ void push(uint64_t key, int lane) {
-    bool pass = key < thr;
-    unsigned b = __ballot_sync(kFull, pass);
-    if (b == 0) return;
-    int cnt = __popc(b);
-    if (nbuf + cnt > L) {
-      flush(lane);
-      pass = key < thr;
-      b = __ballot_sync(kFull, pass);
-      cnt = __popc(b);
+  __device__ __forceinline__ void write_out(int32_t *oi, float *od, int lane) {
+    for (int t = lane; t < k; t += 32) {
+      const uint64_t key = list[t];
+      const bool none = key == kKeyMax;
+      oi[t] = none ? -1 : key_idx(key);
+      od[t] = none ? __int_as_float(0x7f800000) : sqrtf(key_d2(key));
     }
-    if (pass) buf[nbuf + __popc(b & ((1u << lane) - 1))] = key;
-    nbuf += cnt;
+    __syncwarp();
   }
 };
 
-template <int DP4>
+// k-th smallest (1-based rank k, 1 <= k <= n) of the distinct keys s[0..n),
+// by one warp: radix selection with 8-bit digits, starting at the highest bit
+// in which the keys differ; `hist` is a 256-word shared-memory histogram.
+// (Inlined: an out-of-line call spilled the caller's registers around it.)
+__device__ __forceinline__ uint64_t warp_select_kth(const uint64_t *s, int n, int k,
+                                                 uint32_t *hist, int lane) {
+  uint64_t mn = kKeyMax, mx = 0;
+  for (int i = lane; i < n; i += 32) {
+    const uint64_t v = s[i];
+    mn = umin64(mn, v);
+    mx = umax64(mx, v);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = umin64(mn, shfl_xor64(mn, o));
+    mx = umax64(mx, shfl_xor64(mx, o));
+  }
+  if (mn == mx) return mn;
+  const int hb = 63 - __clzll((long long)(mn ^ mx));  // highest differing bit
+  uint64_t known = hb == 63 ? 0ull : (~0ull << (hb + 1));
+  uint64_t prefix = mn & known;
+  uint32_t need = (uint32_t)k;
+  int top = hb + 1;  // bits [0, top) still unknown
+  for (;;) {
+    const int shift = top > 8 ? top - 8 : 0;
+    const uint32_t dmask = (1u << (top - shift)) - 1u;
+    __syncwarp();
+#pragma unroll
+    for (int b = 0; b < 8; b++) hist[b * 32 + lane] = 0;
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) {
+      const uint64_t v = s[i];
+      if ((v & known) == prefix) atomicAdd(&hist[(uint32_t)(v >> shift) & dmask], 1u);
+    }
+    __syncwarp();
+    // bin holding the need-th key: scan the bins 32 at a time
+    uint32_t base = 0, before = 0, cnt_b = 0;
+    int bin = -1;
+#pragma unroll 1
+    for (int j = 0; j < 8 && bin < 0; j++) {
+      const uint32_t h = hist[j * 32 + lane];
+      uint32_t incl = h;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+      }
+      const uint32_t total = __shfl_sync(kFull, incl, 31);
+      if (base + total >= need) {
+        const int wl = __ffs(__ballot_sync(kFull, base + incl >= need)) - 1;
+        bin = j * 32 + wl;
+        before = base + __shfl_sync(kFull, incl - h, wl);
+        cnt_b = __shfl_sync(kFull, h, wl);
+      }
+      base += total;
+    }
+    need -= before;
+    prefix |= (uint64_t)bin << shift;
+    known |= (uint64_t)dmask << shift;
+    if (shift == 0) return prefix;
+    if (cnt_b == 1) {  // the only key with this prefix
+      uint64_t found = 0;
+      bool f = false;
+      for (int i = lane; i < n; i += 32) {
+        const uint64_t v = s[i];
+        if ((v & known) == prefix) {
+          found = v;
+          f = true;
+        }
+      }
+      return shfl64(found, __ffs(__ballot_sync(kFull, f)) - 1);
+    }
+    top = shift;
+  }
+}
+
+// Top-k as an unsorted candidate set in shared memory (capacity 2L).  When it
+// fills, the exact k-th key is found by warp_select_kth, the set is compacted
+// to the k best and the threshold drops to that key; the k results are sorted
+// once, at the end of the query.
+template <int LL>
+struct SelectTopK : TopKBase {
+  static constexpr int L = LL;          // final sort length (pow2 >= k)
+  static constexpr int kCap = 2 * LL;   // candidate capacity
+  static constexpr int kSmemKeys = 2 * LL + 128;  // keys + 256-word histogram
+  uint32_t *hist;
+
+  // Selecting earlier (as soon as k + 32..160 candidates are in) measured
+  // slower on the k = 200 self-join: selections run at capacity only.
+  __device__ __forceinline__ int cap() const { return kCap; }
+
+  __device__ __forceinline__ void init(uint64_t *wsm) {
+    buf = wsm;
+    hist = reinterpret_cast<uint32_t *>(wsm + 2 * LL);
+  }
+
+  __device__ __forceinline__ void reset(float th0, int) { reset_threshold(th0); }
+
+  // Reduce the set to its k smallest keys (no-op with k or fewer).
+  __device__ __forceinline__ void flush(int lane) {
+    if (nbuf <= k) return;
+    __syncwarp();
+    const uint64_t kth = warp_select_kth(buf, nbuf, k, hist, lane);
+    __syncwarp();
+    int w = 0;
+    for (int b0 = 0; b0 < nbuf; b0 += 32) {
+      const int i = b0 + lane;
+      const uint64_t v = i < nbuf ? buf[i] : kKeyMax;
+      const bool keep = i < nbuf && v <= kth;
+      const unsigned bm = __ballot_sync(kFull, keep);
+      __syncwarp();
+      if (keep) buf[w + __popc(bm & ((1u << lane) - 1))] = v;
+      w += __popc(bm);
+    }
+    __syncwarp();
+    nbuf = w;  // == k
+    nlist = k;
+    merges++;
+    thr = kth;
+    theta = sqrtf(key_d2(thr));
+  }
+
+  __device__ __forceinline__ void write_out(int32_t *oi, float *od, int lane) {
+    flush(lane);
+    __syncwarp();
+    for (int i = nbuf + lane; i < LL; i += 32) buf[i] = kKeyMax;
+    __syncwarp();
+    smem_bitonic_sort<LL>(buf, lane);
+    for (int t = lane; t < k; t += 32) {
+      const uint64_t key = buf[t];
+      const bool none = key == kKeyMax;
+      oi[t] = none ? -1 : key_idx(key);
+      od[t] = none ? __int_as_float(0x7f800000) : sqrtf(key_d2(key));
+    }
+    __syncwarp();
+  }
+};
+
+// Offer one key per lane (kKeyMax = nothing); warp-collective.
+template <class TK>
+__device__ __forceinline__ void topk_push(TK &tk, uint64_t key, int lane) {
+  bool pass = key < tk.thr;
+  unsigned b = __ballot_sync(kFull, pass);
+  if (b == 0) return;
+  int cnt = __popc(b);
+  if (tk.nbuf + cnt > tk.cap()) {
+    tk.flush(lane);
+    pass = key < tk.thr;
+    b = __ballot_sync(kFull, pass);
+    cnt = __popc(b);
+  }
+  if (pass) tk.buf[tk.nbuf + __popc(b & ((1u << lane) - 1))] = key;
+  tk.nbuf += cnt;
+  tk.pushed += cnt;
+}
+
+// ---------------------------------------------------------------------------
+// Query rows.  IDXROW: the reference rows carry their original index in the
+// last pad float (d < 4*DP4), which the distance then skips.
+// ---------------------------------------------------------------------------
+template <int DP4, bool IDXROW>
 struct QueryRow {
   float4 v[DP4];
-  __device__ __forceinline__ void load(const float4 *__restrict__ rows,
-                                       int64_t q, int, float4 *) {
+  __device__ __forceinline__ void load(const float4 *__restrict__ rows, int64_t q, int,
+                                       float4 *) {
 #pragma unroll
     for (int c = 0; c < DP4; c++) v[c] = rows[q * DP4 + c];
   }
   __device__ __forceinline__ float dist2(const float4 *__restrict__ r, int) const {
     return dist2_rows<DP4>(v, r);
   }
+  // Member row (already in registers): distance and (IDXROW) the index
+  // stored in the row's last pad float.
+  __device__ __forceinline__ float dist2_member(const float4 (&row)[DP4],
+                                                int32_t *idx) const {
+    float acc = 0.0f;
+#pragma unroll
+    for (int c = 0; c < DP4; c++) {
+      const float4 s = row[c];
+      float t;
+      t = __fsub_rn(v[c].x, s.x); acc = __fmaf_rn(t, t, acc);
+      t = __fsub_rn(v[c].y, s.y); acc = __fmaf_rn(t, t, acc);
+      t = __fsub_rn(v[c].z, s.z); acc = __fmaf_rn(t, t, acc);
+      if (IDXROW && c == DP4 - 1) {
+        *idx = __float_as_int(s.w);
+      } else {
+        t = __fsub_rn(v[c].w, s.w); acc = __fmaf_rn(t, t, acc);
+      }
+    }
+    return acc;
+  }
 };
 
 // Runtime width: the query row lives in the warp's shared-memory slot.
-template <>
-struct QueryRow<0> {
+template <bool IDXROW>
+struct QueryRow<0, IDXROW> {
   const float4 *v;
-  __device__ __forceinline__ void load(const float4 *__restrict__ rows,
-                                       int64_t q, int dp4, float4 *slot) {
-    int lane = threadIdx.x & 31;
+  __device__ __forceinline__ void load(const float4 *__restrict__ rows, int64_t q, int dp4,
+                                       float4 *slot) {
+    const int lane = threadIdx.x & 31;
     __syncwarp();
     for (int c = lane; c < dp4; c += 32) slot[c] = rows[q * dp4 + c];
     __syncwarp();
@@ -170,22 +506,78 @@ struct QueryRow<0> {
   }
 };
 
+// Resident warps per SM the register allocation must allow (compile-time
+// tuning knobs): the scan is latency-bound, so occupancy matters; the
+// register-resident top-k needs more registers per thread.
+#ifndef KNN_TARGET_WARPS_SMEM_TOPK
+#define KNN_TARGET_WARPS_SMEM_TOPK 32
+#endif
+#ifndef KNN_TARGET_WARPS_REG_TOPK
+#define KNN_TARGET_WARPS_REG_TOPK 16
+#endif
+// Load a small member row together with its band distance (before the band
+// test) so both loads are in flight at once.
+#ifndef KNN_EAGER_ROWS
+#define KNN_EAGER_ROWS 1
+#endif
+
+// Traversal choices (compile-time): visit a chunk's clusters nearest d(q,Rs)
+// first, and walk each band outward from d(s,Rs) ~ d(q,Rs).
+#ifndef KNN_ORDER_BY_D
+#define KNN_ORDER_BY_D 1
+#endif
+#ifndef KNN_WALK_OUTWARD
+#define KNN_WALK_OUTWARD 0
+#endif
+
+// Largest list length kept in registers (longer lists live in shared memory).
+#ifndef KNN_REG_TOPK_MAX_L
+#define KNN_REG_TOPK_MAX_L 32
+#endif
+
+// Top-k for lists longer than the register limit: radix-select set
+// (KNN_TOPK_SELECT=1) or sorted shared-memory list with bitonic merges.
+#ifndef KNN_TOPK_SELECT
+#define KNN_TOPK_SELECT 1
+#endif
+
+template <int L>
+using TopKFor = std::conditional_t<
+    (L <= KNN_REG_TOPK_MAX_L), RegTopK<L / 32>,
+    std::conditional_t<(KNN_TOPK_SELECT != 0), SelectTopK<L>, SmemTopK<L>>>;
+
+// Rows of more than 8 floats keep 4+ float4 of the query in registers: those
+// kernels get the lower occupancy target instead of spilling.
 template <int DP4, int L, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32)
+constexpr int scan_min_blocks() {
+  return (((L <= KNN_REG_TOPK_MAX_L && L > 32) || DP4 == 0 || DP4 >= 4)
+              ? KNN_TARGET_WARPS_REG_TOPK
+              : KNN_TARGET_WARPS_SMEM_TOPK) /
+         WARPS;
+}
+
+template <int DP4, bool IDXROW, int L, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, L, WARPS>()))
     scan_kernel(const ScanArgs a) {
+  using TK = TopKFor<L>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int dp4 = DP4 > 0 ? DP4 : a.dp4;
-  uint64_t *wsm = reinterpret_cast<uint64_t *>(smem_raw) + (size_t)w * 2 * L;
-  float4 *qslot = reinterpret_cast<float4 *>(
-                      reinterpret_cast<uint64_t *>(smem_raw) + (size_t)WARPS * 2 * L) +
+  uint64_t *keys_base = reinterpret_cast<uint64_t *>(smem_raw);
+  float4 *qslot = reinterpret_cast<float4 *>(keys_base + (size_t)WARPS * TK::kSmemKeys) +
                   (size_t)w * (DP4 > 0 ? 0 : a.dp4);
-  WarpTopK<L> tk;
-  tk.list = wsm;
-  tk.buf = wsm + L;
+  TK tk;
+  tk.init(keys_base + (size_t)w * TK::kSmemKeys);
   tk.k = a.k;
   const float tol = bound_tol(a.d);
-  unsigned long long evals = 0, visited = 0, pruned = 0;
+  unsigned evals = 0, visited = 0, pruned = 0;
+  // small rows: load the member row together with its band distance
+  constexpr bool kEagerRow = KNN_EAGER_ROWS && (DP4 > 0 && DP4 <= 2);
+  // statistics: per-lane 32-bit counts folded once per query into per-block
+  // shared counters, added to the global ones at exit
+  __shared__ unsigned long long blk_ctr[5];
+  if (threadIdx.x < 5) blk_ctr[threadIdx.x] = 0;
+  __syncthreads();
 
   for (;;) {
     long long slot = 0;
@@ -194,9 +586,52 @@ __global__ void __launch_bounds__(WARPS * 32)
     if (slot >= a.m) break;
     const int64_t q = a.qorder[slot];
     const int qc = a.slot_cl[slot];
-    QueryRow<DP4> qr;
+    QueryRow<DP4, IDXROW> qr;
     qr.load(a.qrows, q, dp4, qslot);
     tk.reset(a.theta0[qc], lane);
+
+    // one band step: lane's member p of the cluster at `start`, kept when
+    // its distance to the representative lies in [lo_v, hi_v]
+    auto step = [&](int start, int p, bool valid, float lo_v, float hi_v) -> float {
+      const int64_t gp = (int64_t)start + p;
+      float dsv = 0.0f, v = 0.0f;
+      int32_t idx = 0;
+      bool inb;
+      if constexpr (kEagerRow) {
+        // small rows: issue the row load together with the band distance
+        float4 row[DP4];
+        if (valid) {
+#pragma unroll
+          for (int c = 0; c < DP4; c++) row[c] = a.srows[gp * DP4 + c];
+          dsv = a.sdist[gp];
+        }
+        inb = valid && dsv >= lo_v && dsv <= hi_v;
+        if (inb) v = qr.dist2_member(row, &idx);
+      } else if constexpr (DP4 > 0) {
+        dsv = valid ? a.sdist[gp] : 0.0f;
+        inb = valid && dsv >= lo_v && dsv <= hi_v;
+        if (inb) {
+          float4 row[DP4];
+#pragma unroll
+          for (int c = 0; c < DP4; c++) row[c] = a.srows[gp * DP4 + c];
+          v = qr.dist2_member(row, &idx);
+        }
+      } else {
+        dsv = valid ? a.sdist[gp] : 0.0f;
+        inb = valid && dsv >= lo_v && dsv <= hi_v;
+        if (inb) v = qr.dist2(a.srows + gp * dp4, dp4);
+      }
+      uint64_t key = kKeyMax;
+      if (inb) {
+        evals++;
+        if (v <= key_d2(tk.thr)) {
+          if (!IDXROW) idx = a.sidx[gp];
+          key = make_key(v, idx);
+        }
+      }
+      topk_push(tk, key, lane);
+      return dsv;
+    };
 
     const int nr = a.rlen[qc];
     const int32_t *rl = a.rlist + (int64_t)qc * a.Rs;
@@ -208,17 +643,37 @@ __global__ void __launch_bounds__(WARPS * 32)
       if (j < nr) {
         rs = rl[j];
         D = sqrtf(qr.dist2(a.sreps + (int64_t)rs * dp4, dp4));
-        float th = tk.theta;
-        float slack = tol * (2.0f * D + 2.0f * th);
+        const float th = tk.theta;
+        const float slack = tol * (2.0f * D + 2.0f * th);
         alive = !(D - a.cmax[rs] > th + slack) && !(D + th + slack < a.cmin[rs]);
         if (!alive) pruned++;
       }
-      unsigned mask = __ballot_sync(kFull, alive);
-      while (mask) {
-        const int src = __ffs(mask) - 1;
-        mask &= mask - 1;
-        const int c = __shfl_sync(kFull, rs, src);
+      // visit this chunk's surviving clusters: in list order (by rep-rep
+      // distance) or, with KNN_ORDER_BY_D, nearest d(q, Rs) first
+      unsigned amask = __ballot_sync(kFull, alive);
+      float dkey = alive ? D : __int_as_float(0x7f800000);
+      while (amask) {
+        int src = __ffs(amask) - 1;
+#if KNN_ORDER_BY_D
+        if (amask & (amask - 1)) {
+          float mv = dkey;
+          int ml = lane;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            const float ov = __shfl_xor_sync(kFull, mv, o);
+            const int ol = __shfl_xor_sync(kFull, ml, o);
+            if (ov < mv || (ov == mv && ol < ml)) {
+              mv = ov;
+              ml = ol;
+            }
+          }
+          src = ml;
+        }
+        if (lane == src) dkey = __int_as_float(0x7f800000);
+#endif
+        amask &= ~(1u << src);
         const float Dc = __shfl_sync(kFull, D, src);
+        const int c = __shfl_sync(kFull, rs, src);
         float th = tk.theta;
         float slack = tol * (2.0f * Dc + 2.0f * th);
         if (Dc - a.cmax[c] > th + slack || Dc + th + slack < a.cmin[c]) {
@@ -226,65 +681,91 @@ __global__ void __launch_bounds__(WARPS * 32)
           continue;
         }
         if (lane == 0) visited++;
-        const int start = a.soff[c], end = a.soff[c + 1];
-        const int lo = warp_lower_bound(a.sdist + start, end - start,
-                                        Dc - th - slack, lane);
-        for (int p0 = start + lo; p0 < end; p0 += 32) {
-          const int p = p0 + lane;
+        const int start = a.soff[c];
+        const int n_c = a.soff[c + 1] - start;
+#if KNN_WALK_OUTWARD
+        // members below `mid` have d(s,Rs) < Dc, from `mid` on >= Dc; walk
+        // outward from there, alternately up and down
+        const int mid = warp_lower_bound(a.sdist + start, n_c, Dc, lane);
+        int up = mid, dn = mid;
+        bool go_up = up < n_c, go_dn = dn > 0;
+        while (go_up || go_dn) {
+          if (go_up) {
+            th = tk.theta;
+            slack = tol * (2.0f * Dc + 2.0f * th);
+            const float hi_v = Dc + th + slack;
+            const int p = up + lane;
+            const bool valid = p < n_c;
+            const float dsv = step(start, p, valid, -1.0f, hi_v);
+            const bool past = !valid || dsv > hi_v;
+            up += 32;
+            if (__shfl_sync(kFull, past, 31) || up >= n_c) go_up = false;
+          }
+          if (go_dn) {
+            th = tk.theta;
+            slack = tol * (2.0f * Dc + 2.0f * th);
+            const float lo_v = Dc - th - slack;
+            const int p = dn - 32 + lane;
+            const bool valid = p >= 0;
+            const float dsv = step(start, p, valid, lo_v, __int_as_float(0x7f800000));
+            const bool past = !valid || dsv < lo_v;
+            dn -= 32;
+            if (__shfl_sync(kFull, past, 0) || dn <= 0) go_dn = false;
+          }
+        }
+#else
+        // one direction: from the lower band edge up
+        const int lo = warp_lower_bound(a.sdist + start, n_c, Dc - th - slack, lane);
+        for (int p0 = lo; p0 < n_c; p0 += 32) {
           th = tk.theta;
           slack = tol * (2.0f * Dc + 2.0f * th);
-          const float up = Dc + th + slack, dn = Dc - th - slack;
-          const bool valid = p < end;
-          const float dsv = valid ? a.sdist[p] : 0.0f;
-          const bool inb = valid && dsv <= up && dsv >= dn;
-          uint64_t key = kKeyMax;
-          if (inb) {
-            const float v = qr.dist2(a.srows + (int64_t)p * dp4, dp4);
-            evals++;
-            if (v <= key_d2(tk.thr)) key = make_key(v, a.sidx[p]);
-          }
-          tk.push(key, lane);
-          const bool past = !valid || dsv > up;
+          const float hi_v = Dc + th + slack, lo_v = Dc - th - slack;
+          const int p = p0 + lane;
+          const bool valid = p < n_c;
+          const float dsv = step(start, p, valid, lo_v, hi_v);
+          const bool past = !valid || dsv > hi_v;
           if (__shfl_sync(kFull, past, 31)) break;
         }
+#endif
       }
     }
     tk.flush(lane);
-    int32_t *oi = a.out_idx + q * a.k;
-    float *od = a.out_dist + q * a.k;
-    for (int t = lane; t < a.k; t += 32) {
-      uint64_t key = tk.list[t];
-      bool none = key == kKeyMax;
-      oi[t] = none ? -1 : key_idx(key);
-      od[t] = none ? __int_as_float(0x7f800000) : sqrtf(key_d2(key));
+    tk.write_out(a.out_idx + q * a.k, a.out_dist + q * a.k, lane);
+    if (a.counters) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        evals += __shfl_xor_sync(kFull, evals, o);
+        visited += __shfl_xor_sync(kFull, visited, o);
+        pruned += __shfl_xor_sync(kFull, pruned, o);
+      }
+      if (lane == 0) {
+        atomicAdd(&blk_ctr[0], (unsigned long long)evals);
+        atomicAdd(&blk_ctr[1], (unsigned long long)visited);
+        atomicAdd(&blk_ctr[2], (unsigned long long)pruned);
+        atomicAdd(&blk_ctr[3], (unsigned long long)tk.pushed);
+        atomicAdd(&blk_ctr[4], (unsigned long long)tk.merges);
+      }
     }
-    __syncwarp();
+    evals = visited = pruned = 0;
+    tk.pushed = tk.merges = 0;
   }
-  // one atomic per warp for each statistic
-  for (int o = 16; o > 0; o >>= 1) {
-    evals += __shfl_xor_sync(kFull, evals, o);
-    visited += __shfl_xor_sync(kFull, visited, o);
-    pruned += __shfl_xor_sync(kFull, pruned, o);
-  }
-  if (lane == 0 && a.counters) {
-    atomicAdd(a.counters + 0, evals);
-    atomicAdd(a.counters + 1, visited);
-    atomicAdd(a.counters + 2, pruned);
-  }
+  __syncthreads();
+  if (a.counters && threadIdx.x < 5) atomicAdd(a.counters + threadIdx.x, blk_ctr[threadIdx.x]);
 }
 
-template <int DP4, int L, int WARPS>
+template <int DP4, bool IDXROW, int L, int WARPS>
 static int launch_scan_t(const ScanArgs &a, int num_sms, cudaStream_t s) {
-  size_t smem = (size_t)WARPS * 2 * L * sizeof(uint64_t) +
-                (DP4 > 0 ? 0 : (size_t)WARPS * a.dp4 * sizeof(float4));
-  auto kern = scan_kernel<DP4, L, WARPS>;
+  using TK = TopKFor<L>;
+  const size_t smem = (size_t)WARPS * TK::kSmemKeys * sizeof(uint64_t) +
+                      (DP4 > 0 ? 0 : (size_t)WARPS * a.dp4 * sizeof(float4));
+  auto kern = scan_kernel<DP4, IDXROW, L, WARPS>;
   if (smem > 48 * 1024)
     KNN_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
   int per_sm = 0;
   KNN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, smem));
   if (per_sm < 1) per_sm = 1;
-  int64_t want = (a.m + WARPS - 1) / WARPS;
+  const int64_t want = (a.m + WARPS - 1) / WARPS;
   int64_t grid = (int64_t)num_sms * per_sm;
   if (grid > want) grid = want;
   if (grid < 1) grid = 1;
@@ -293,24 +774,28 @@ static int launch_scan_t(const ScanArgs &a, int num_sms, cudaStream_t s) {
   return KNN_OK;
 }
 
-template <int DP4>
+template <int DP4, bool IDXROW>
 static int launch_scan_l(const ScanArgs &a, int num_sms, cudaStream_t s) {
-  if (a.k <= 32) return launch_scan_t<DP4, 32, 8>(a, num_sms, s);
-  if (a.k <= 64) return launch_scan_t<DP4, 64, 8>(a, num_sms, s);
-  if (a.k <= 128) return launch_scan_t<DP4, 128, 8>(a, num_sms, s);
-  if (a.k <= 256) return launch_scan_t<DP4, 256, 8>(a, num_sms, s);
-  if (a.k <= 512) return launch_scan_t<DP4, 512, 4>(a, num_sms, s);
-  return launch_scan_t<DP4, 1024, 4>(a, num_sms, s);
+  if (a.k <= 32) return launch_scan_t<DP4, IDXROW, 32, 8>(a, num_sms, s);
+  if (a.k <= 64) return launch_scan_t<DP4, IDXROW, 64, 8>(a, num_sms, s);
+  if (a.k <= 128) return launch_scan_t<DP4, IDXROW, 128, 8>(a, num_sms, s);
+  if (a.k <= 256) return launch_scan_t<DP4, IDXROW, 256, 8>(a, num_sms, s);
+  if (a.k <= 512) return launch_scan_t<DP4, IDXROW, 512, 4>(a, num_sms, s);
+  return launch_scan_t<DP4, IDXROW, 1024, 4>(a, num_sms, s);
 }
 
 int launch_scan(const ScanArgs &a, int num_sms, cudaStream_t s) {
   if (a.m == 0) return KNN_OK;
   switch (a.dp4_tmpl) {
-    case 1: return launch_scan_l<1>(a, num_sms, s);
-    case 2: return launch_scan_l<2>(a, num_sms, s);
-    case 4: return launch_scan_l<4>(a, num_sms, s);
-    case 8: return launch_scan_l<8>(a, num_sms, s);
-    default: return launch_scan_l<0>(a, num_sms, s);
+    case 1: return a.idx_in_row ? launch_scan_l<1, true>(a, num_sms, s)
+                                : launch_scan_l<1, false>(a, num_sms, s);
+    case 2: return a.idx_in_row ? launch_scan_l<2, true>(a, num_sms, s)
+                                : launch_scan_l<2, false>(a, num_sms, s);
+    case 4: return a.idx_in_row ? launch_scan_l<4, true>(a, num_sms, s)
+                                : launch_scan_l<4, false>(a, num_sms, s);
+    case 8: return a.idx_in_row ? launch_scan_l<8, true>(a, num_sms, s)
+                                : launch_scan_l<8, false>(a, num_sms, s);
+    default: return launch_scan_l<0, false>(a, num_sms, s);
   }
 }
 

@@ -31,6 +31,8 @@ class JoinStats:
     clusters_visited: int
     clusters_pruned: int
     refine_rechecks: int
+    topk_candidates: int
+    topk_merges: int
     ms_build: float
     ms_search: float
     ms_total: float

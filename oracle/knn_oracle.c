@@ -32,6 +32,7 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -297,7 +298,17 @@ typedef struct oracle_port_stats {
   int64_t clusters_pruned;
   int32_t qreps_trial;
   int32_t sreps_trial;
+  double build_seconds; /* representatives .. cluster filter */
+  double scan_seconds;  /* per-query scan of the requested rows */
 } oracle_port_stats;
+
+static double wall_seconds(void) {
+#ifdef _OPENMP
+  return omp_get_wtime();
+#else
+  return (double)clock() / CLOCKS_PER_SEC;
+#endif
+}
 
 /*
  * The reference's pruned join restated on the CPU.  Queries processed are
@@ -317,6 +328,7 @@ int oracle_port_join(const float *q, int64_t m, const float *r, int64_t n,
   if (!qrows) nq = m;
   int nt = resolve_threads(nthreads);
   const float tol = port_tol(d);
+  double t_start = wall_seconds();
 
   /* representatives (knnjoin.cu:195-239) */
   int32_t *qrow = (int32_t *)malloc(sizeof(int32_t) * qreps);
@@ -445,6 +457,7 @@ int oracle_port_join(const float *q, int64_t m, const float *r, int64_t n,
    * clusters nearest first; inside a cluster only members whose distance to
    * the representative lies within theta of d(q,Rs) can be closer than the
    * running k-th neighbour; insertion into a sorted list of k. */
+  double t_built = wall_seconds();
   int64_t evals = 0, visited = 0, pruned = 0;
   int64_t t;
 #pragma omp parallel for schedule(dynamic, 16) num_threads(nt) \
@@ -518,7 +531,10 @@ int oracle_port_join(const float *q, int64_t m, const float *r, int64_t n,
     free(ld);
     free(li);
   }
+  double t_done = wall_seconds();
   if (st) {
+    st->build_seconds = t_built - t_start;
+    st->scan_seconds = t_done - t_built;
     st->dist_evals = evals;
     st->clusters_visited = visited;
     st->clusters_pruned = pruned;

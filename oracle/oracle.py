@@ -31,6 +31,8 @@ class PortStats(ctypes.Structure):
         ("clusters_pruned", ctypes.c_int64),
         ("qreps_trial", ctypes.c_int32),
         ("sreps_trial", ctypes.c_int32),
+        ("build_seconds", ctypes.c_double),
+        ("scan_seconds", ctypes.c_double),
     ]
 
 
