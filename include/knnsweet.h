@@ -140,6 +140,35 @@ int knn_backward_device(const float *q, int64_t m, const float *r, int64_t n,
                         void *stream);
 
 /*
+ * Allocation-free variant of knn_join_device.  It has no counterpart in the
+ * reference (which cudaMallocs everything and never frees it).
+ *
+ * For callers that may not allocate device memory: applications that reserve
+ * the whole GPU for their own memory manager at start-up, and code that must
+ * not allocate once running because cudaMalloc / cudaFree can block and
+ * synchronise the device.  The caller passes device inputs and outputs
+ * exactly as for knn_join_device; every other buffer the join needs is carved
+ * from one array of KNN_NOALLOC_SCRATCH_BYTES compiled into the library, and
+ * the call makes no cudaMalloc, cudaFree or other allocating call.
+ *  - Limit: a join whose scratch exceeds KNN_NOALLOC_SCRATCH_BYTES (32 MiB;
+ *    about 250,000 points for a d = 3 self-join with 800 representatives) is
+ *    rejected with KNN_EINVAL and a message giving the bytes it would need.
+ *  - Every GPU that loads the library holds the array until the process
+ *    exits.  The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress) with that device current; make that first call
+ *    before any stream capture.
+ *  - All calls on a device share the one array, and it keeps the previous
+ *    call's contents: calls that overlap on the GPU (different streams, or
+ *    host threads racing) corrupt each other.  Serialise them.
+ *  - No statistics: the stats-filling path of knn_join_device creates events.
+ */
+#define KNN_NOALLOC_SCRATCH_BYTES (32u << 20)
+int knn_join_device_noalloc(const float *q, int64_t m, const float *r, int64_t n,
+                            int32_t d, int32_t k, int32_t *out_idx,
+                            float *out_dist, const knn_options *opt,
+                            void *stream);
+
+/*
  * Returns the device scratch memory the library keeps cached between calls
  * (one stream-ordered pool per device; no reference counterpart: the
  * reference never frees its device memory).  Memory still in use by calls in

@@ -74,6 +74,8 @@ SIGNATURES = {
                                      _vp, _vp, _vp]),
     "knn_pack_indexdist": (None, [_vp, _vp, _c_i64, _vp]),
     "knn_trim_memory": (_c_int, []),
+    "knn_join_device_noalloc": (_c_int, [_vp, _c_i64, _vp, _c_i64, _c_i32, _c_i32, _vp, _vp,
+                                         ctypes.POINTER(KnnOptions), _vp]),
 }
 
 _lock = threading.Lock()

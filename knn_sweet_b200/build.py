@@ -32,7 +32,7 @@ NVCC_FLAGS = ARCH + [
     "-Xcompiler", "-Wall", "-I", str(ROOT / "include"),
 ]
 
-CU_SOURCES = ["api.cu", "build_index.cu", "scan.cu", "backward.cu"]
+CU_SOURCES = ["api.cu", "build_index.cu", "scan.cu", "backward.cu", "noalloc.cu"]
 HEADERS = ["common.cuh", "kernels.cuh", "glibc_rand.h"]
 
 
