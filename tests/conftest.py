@@ -13,6 +13,14 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built libknnsweet.so")
 
 
+def pytest_sessionstart(session):
+    """Build the library and the command line in-tree when they are missing
+    (nvcc cross-compiles without a GPU)."""
+    from knn_sweet_b200 import build as kb
+    if not kb.LIB.exists() or not kb.CLI.exists():
+        kb.build()
+
+
 @pytest.fixture(scope="session")
 def oracle():
     from oracle import oracle as o
