@@ -133,6 +133,21 @@ def test_rep_counts_do_not_change_result(cuda_device):
         assert np.array_equal(base[0], got[0]) and np.array_equal(base[1], got[1])
 
 
+def test_matches_reference_program_output(cuda_device):
+    """Against the reference's own CUDA program's result on the same points
+    (tests/golden/ref_skin2000_k32.npz): identical sorted distances, identical
+    index sets below the K-th distance, the same number of points at it."""
+    from pathlib import Path
+    z = np.load(Path(__file__).resolve().parent / "golden" / "ref_skin2000_k32.npz")
+    x, k, reps = z["x"], int(z["k"]), int(z["reps"])
+    idx, dist = knnjoin(x, None, k, qreps=reps, sreps=reps)
+    ri, rd = z["ref_idx"], z["ref_dist"]
+    assert np.array_equal(dist, np.sort(rd, axis=1))
+    for i in range(x.shape[0]):
+        kth = dist[i, -1]
+        assert set(idx[i][dist[i] < kth]) == set(ri[i][rd[i] < kth])
+
+
 def test_full_size_skin_selfjoin_properties(cuda_device, oracle):
     """The full self-join workload (245,057 points, k=200, 800/800 reps):
     size-independent properties on all rows, oracle comparison on a sample."""

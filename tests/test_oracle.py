@@ -86,6 +86,34 @@ def test_port_float_data(oracle):
     np.testing.assert_allclose(pd, bd, rtol=1e-5)
 
 
+def test_oracle_pinned_to_reference_output(oracle):
+    """tests/golden/ref_skin2000_k32.npz holds the reference's own CUDA program's
+    full result (2,000 skin-like points joined with themselves, K=32, 50/50
+    representatives; made on a B200 by `oracle/compare_ref.py --golden`).  The
+    FP64 oracle must reproduce its neighbour distances exactly and its index
+    sets up to the order of points tied at the K-th distance (the reference's
+    tie order is not deterministic)."""
+    z = np.load(GOLDEN / "ref_skin2000_k32.npz")
+    x, k = z["x"], int(z["k"])
+    ri, rd = z["ref_idx"], z["ref_dist"]
+    assert np.array_equal(x, data.skin_like(x.shape[0], seed=int(z["seed"])))
+    oi, od = oracle.bruteforce_f64(x, x, k)
+    od32 = od.astype(np.float32)
+    assert np.array_equal(np.sort(rd, axis=1), od32)
+    for i in range(x.shape[0]):
+        kth = od32[i, -1]
+        assert set(ri[i][rd[i] < kth]) == set(oi[i][od32[i] < kth]), i
+        # at the K-th distance both chose the same number of tied points
+        assert np.count_nonzero(rd[i] == kth) == np.count_nonzero(od32[i] == kth)
+
+
+def test_port_matches_reference_output(oracle):
+    z = np.load(GOLDEN / "ref_skin2000_k32.npz")
+    x, k, reps = z["x"], int(z["k"]), int(z["reps"])
+    pi, pd, _ = oracle.port_join(x, x, k, reps, reps)
+    assert np.array_equal(np.sort(z["ref_dist"], axis=1), pd)
+
+
 def test_select_reps_uses_seeded_draw(oracle):
     x = data.skin_like(5000, seed=2)
     rows, trial = oracle.select_reps(x, 50, seed=2015, trials=10)
