@@ -48,6 +48,9 @@ extern "C" {
 #define KNN_BF16_REFINE 1 /* BF16 tensor-core distances, FP32 re-rank of the
                              top k+margin, FP64 re-check of k-th ties         */
 
+/* Option flags. */
+#define KNN_SQUARED_DIST 1 /* out_dist holds squared distances |q - r|^2     */
+
 /* Limits. */
 #define KNN_MAX_K 1024    /* the reference allows K <= 1000 (knnjoin.cu:774) */
 #define KNN_MAX_REPS 8192
@@ -67,7 +70,7 @@ typedef struct knn_options {
   int32_t precision;  /* KNN_FP32 or KNN_BF16_REFINE                          */
   int32_t margin;     /* extra candidates re-ranked by the BF16 form         */
   int32_t autotune;   /* batched form: pick tiles per cloud-size bucket      */
-  int32_t flags;      /* reserved, must be 0                                 */
+  int32_t flags;      /* KNN_SQUARED_DIST or 0                               */
 } knn_options;
 
 /*

@@ -1,0 +1,75 @@
+"""Differentiable kNN squared distances over the C ABI.
+
+``knn_dist2(queries, sources, k)`` returns, for every query row, its k nearest
+source rows (``idx``) and the squared distances ``d2[i, t] = |q_i - s_idx|^2``
+as a tensor that is differentiable with respect to both point sets.  The
+neighbour sets are constants of the forward pass (the join is piecewise
+constant in the coordinates); the backward pass is the hand-written kernel
+``knn_backward_device`` (csrc/backward.cu):
+
+    grad_q[i] += 2 g (q_i - s_j),      grad_s[j] -= 2 g (q_i - s_j).
+
+The reference computes no gradient; this is the "differentiation form" of
+the join (e.g. kNN Chamfer losses between point clouds).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+from .join import knnjoin
+
+
+def _ptr(t: torch.Tensor) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class _KnnDist2(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, queries, sources, k, qreps, sreps):
+        q = queries.detach().contiguous()
+        s = sources.detach().contiguous()
+        # the join writes the squared distances it ranked by (FP32, summed in
+        # dimension order); missing neighbours are (-1, +inf)
+        idx, d2 = knnjoin(q, s, k, qreps=qreps, sreps=sreps, squared=True)
+        ctx.save_for_backward(q, s, idx)
+        ctx.mark_non_differentiable(idx)
+        return d2, idx
+
+    @staticmethod
+    def backward(ctx, grad_d2, _grad_idx):
+        q, s, idx = ctx.saved_tensors
+        m, d = q.shape
+        n = s.shape[0]
+        k = idx.shape[1]
+        g = grad_d2.contiguous().to(torch.float32)
+        g = torch.where(idx >= 0, g, torch.zeros_like(g))
+        grad_q = torch.zeros_like(q)
+        grad_s = torch.zeros_like(s) if ctx.needs_input_grad[1] else None
+        lib = _lib.load()
+        with torch.cuda.device(q.device):
+            stream = ctypes.c_void_p(torch.cuda.current_stream(q.device).cuda_stream)
+            rc = lib.knn_backward_device(_ptr(q), m, _ptr(s), n, d, k, _ptr(idx), _ptr(g),
+                                         _ptr(grad_q),
+                                         _ptr(grad_s) if grad_s is not None else None, stream)
+        _lib.check(rc)
+        return grad_q, grad_s, None, None, None
+
+
+def knn_dist2(queries: torch.Tensor, sources: torch.Tensor, k: int, *, qreps: int = 0,
+              sreps: int = 0):
+    """(d2, idx): k nearest squared distances (differentiable) and indices."""
+    if not (queries.is_cuda and sources.is_cuda):
+        raise ValueError("knn_dist2 needs CUDA tensors")
+    return _KnnDist2.apply(queries, sources, k, qreps, sreps)
+
+
+def knn_chamfer(x: torch.Tensor, y: torch.Tensor, k: int = 1) -> torch.Tensor:
+    """Sum of the k nearest squared distances in both directions:
+    sum_i sum_t |x_i - y_nn(i,t)|^2 + sum_j sum_t |y_j - x_nn(j,t)|^2
+    (k = 1 is the Chamfer distance)."""
+    dxy, _ = knn_dist2(x, y, k)
+    dyx, _ = knn_dist2(y, x, k)
+    return dxy.sum() + dyx.sum()

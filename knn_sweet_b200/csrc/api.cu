@@ -231,8 +231,8 @@ int check_options(const knn_options *opt, knn_options *o) {
     set_error("margin must be in [0, 4096]");
     return KNN_EINVAL;
   }
-  if (o->flags != 0) {
-    set_error("flags must be 0");
+  if ((o->flags & ~KNN_SQUARED_DIST) != 0) {
+    set_error("unknown flags 0x%x", o->flags);
     return KNN_EINVAL;
   }
   return KNN_OK;
@@ -382,6 +382,7 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
   a.dp4_tmpl = tmpl;
   a.k = k;
   a.idx_in_row = idx_in_row;
+  a.squared = (o.flags & KNN_SQUARED_DIST) != 0;
   a.sreps = sset.reps;
   a.srows = srows;
   a.sdist = sdist;

@@ -14,6 +14,7 @@ struct ScanArgs {
   int64_t m;
   int d, dp4, dp4_tmpl, k;
   bool idx_in_row;          // srows carry the index in their last pad float
+  bool squared;             // write squared distances instead of distances
   const float4 *sreps;      // Rs x dp4 reference representatives
   const float4 *srows;      // n x dp4, cluster-contiguous, ascending d(s,Rs)
   const float *sdist;       // n: d(s, Rs) in the same order

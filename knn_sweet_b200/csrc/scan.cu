@@ -181,7 +181,7 @@ struct RegTopK : TopKBase {
   }
 
   // Writes the k results (through the buffer for coalesced stores).
-  __device__ __forceinline__ void write_out(int32_t *oi, float *od, int lane) {
+  __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int lane) {
     __syncwarp();
 #pragma unroll
     for (int j = 0; j < E; j++) buf[E * lane + j] = v[j];
@@ -190,7 +190,7 @@ struct RegTopK : TopKBase {
       const uint64_t key = buf[t];
       const bool none = key == kKeyMax;
       oi[t] = none ? -1 : key_idx(key);
-      od[t] = none ? __int_as_float(0x7f800000) : sqrtf(key_d2(key));
+      od[t] = none ? __int_as_float(0x7f800000) : (squared ? key_d2(key) : sqrtf(key_d2(key)));
     }
     __syncwarp();
   }
@@ -285,12 +285,12 @@ struct SmemTopK : TopKBase {
     }
   }
 
-  __device__ __forceinline__ void write_out(int32_t *oi, float *od, int lane) {
+  __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int lane) {
     for (int t = lane; t < k; t += 32) {
       const uint64_t key = list[t];
       const bool none = key == kKeyMax;
       oi[t] = none ? -1 : key_idx(key);
-      od[t] = none ? __int_as_float(0x7f800000) : sqrtf(key_d2(key));
+      od[t] = none ? __int_as_float(0x7f800000) : (squared ? key_d2(key) : sqrtf(key_d2(key)));
     }
     __syncwarp();
   }
@@ -418,7 +418,7 @@ struct SelectTopK : TopKBase {
     theta = sqrtf(key_d2(thr));
   }
 
-  __device__ __forceinline__ void write_out(int32_t *oi, float *od, int lane) {
+  __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int lane) {
     flush(lane);
     __syncwarp();
     for (int i = nbuf + lane; i < LL; i += 32) buf[i] = kKeyMax;
@@ -428,7 +428,7 @@ struct SelectTopK : TopKBase {
       const uint64_t key = buf[t];
       const bool none = key == kKeyMax;
       oi[t] = none ? -1 : key_idx(key);
-      od[t] = none ? __int_as_float(0x7f800000) : sqrtf(key_d2(key));
+      od[t] = none ? __int_as_float(0x7f800000) : (squared ? key_d2(key) : sqrtf(key_d2(key)));
     }
     __syncwarp();
   }
@@ -730,7 +730,7 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, L, WARPS>())
       }
     }
     tk.flush(lane);
-    tk.write_out(a.out_idx + q * a.k, a.out_dist + q * a.k, lane);
+    tk.write_out(a.out_idx + q * a.k, a.out_dist + q * a.k, a.squared, lane);
     if (a.counters) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {

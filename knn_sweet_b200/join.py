@@ -42,8 +42,11 @@ class JoinStats:
     reserved: int = 0
 
 
-def _options(qreps, sreps, seed, rep_trials, precision, margin) -> _lib.KnnOptions:
+def _options(qreps, sreps, seed, rep_trials, precision, margin,
+             squared=False) -> _lib.KnnOptions:
     o = _lib.default_options()
+    if squared:
+        o.flags |= _lib.KNN_SQUARED_DIST
     o.qreps = int(qreps)
     o.sreps = int(sreps)
     o.seed = int(seed) & 0xFFFFFFFF
@@ -65,7 +68,7 @@ def _is_torch(x) -> bool:
 
 def knnjoin(queries, sources=None, k: int = 200, *, qreps: int = 0, sreps: int = 0,
             seed: int = 2015, rep_trials: int = 10, precision: str = "fp32",
-            margin: int = 32, stats: bool = False, out=None):
+            margin: int = 32, stats: bool = False, out=None, squared: bool = False):
     """Exact k nearest neighbours of every query row among the source rows.
 
     queries: (m, d) float32; sources: (n, d) float32 or None for a self-join
@@ -74,10 +77,10 @@ def knnjoin(queries, sources=None, k: int = 200, *, qreps: int = 0, sreps: int =
     ties to the lower source row; slots beyond n hold (-1, inf).  With
     stats=True a JoinStats is returned as a third element.  `out` may give
     preallocated (idx, dist) arrays of the input's kind (e.g. pinned host
-    memory for the host path).
+    memory for the host path).  squared=True returns squared distances.
     """
     lib = _lib.load()
-    opt = _options(qreps, sreps, seed, rep_trials, precision, margin)
+    opt = _options(qreps, sreps, seed, rep_trials, precision, margin, squared)
     st = _lib.KnnStats()
     stp = ctypes.byref(st) if stats else None
     if _is_torch(queries) and queries.is_cuda:
