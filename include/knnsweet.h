@@ -50,6 +50,10 @@ extern "C" {
 
 /* Option flags. */
 #define KNN_SQUARED_DIST 1 /* out_dist holds squared distances |q - r|^2     */
+#define KNN_NO_TENSOR_CORES 2 /* CUDA-core FP32 kernels only (for comparison):
+                             the point-to-representative assignment of rows
+                             with d >= 16 otherwise runs on tcgen05 in BF16
+                             (results are identical; only clusters differ)  */
 
 /* Limits. */
 #define KNN_MAX_K 1024    /* the reference allows K <= 1000 (knnjoin.cu:774) */
@@ -70,7 +74,7 @@ typedef struct knn_options {
   int32_t precision;  /* KNN_FP32 or KNN_BF16_REFINE                          */
   int32_t margin;     /* extra candidates re-ranked by the BF16 form         */
   int32_t autotune;   /* batched form: pick tiles per cloud-size bucket      */
-  int32_t flags;      /* KNN_SQUARED_DIST or 0                               */
+  int32_t flags;      /* KNN_SQUARED_DIST | KNN_NO_TENSOR_CORES, or 0        */
 } knn_options;
 
 /*

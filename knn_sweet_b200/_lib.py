@@ -20,6 +20,7 @@ KNN_EINTERNAL = -5
 KNN_FP32 = 0
 KNN_BF16_REFINE = 1
 KNN_SQUARED_DIST = 1
+KNN_NO_TENSOR_CORES = 2
 KNN_MAX_K = 1024
 KNN_MAX_REPS = 8192
 

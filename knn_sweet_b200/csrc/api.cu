@@ -174,8 +174,9 @@ struct ClusterSet {
   int32_t *off = nullptr;     // R + 1
 };
 
-int build_clusters(Arena &ar, const float4 *rows, int64_t n, int dp4s, int R,
-                   uint32_t seed, int trials, cudaStream_t s, ClusterSet *cs) {
+int build_clusters(Arena &ar, const float4 *rows, int64_t n, int d, int dp4s, int R,
+                   uint32_t seed, int trials, bool use_tc, int *err, cudaStream_t s,
+                   ClusterSet *cs) {
   cs->R = R;
   // representative draw on the host: trials x R indices rand() % n
   std::vector<int32_t> cand((size_t)trials * R);
@@ -194,7 +195,14 @@ int build_clusters(Arena &ar, const float4 *rows, int64_t n, int dp4s, int R,
   float *dr;
   KNN_TRY(ar.alloc(&cl, (size_t)n));
   KNN_TRY(ar.alloc(&dr, (size_t)n));
-  KNN_TRY(launch_assign(rows, n, dp4s, cs->reps, R, cl, dr, s));
+  if (use_tc && assign_tc_supported(d)) {
+    // BF16 tensor-core arg-min, then the exact FP32 distance to the winner
+    unsigned char *tc_scratch;
+    KNN_TRY(ar.alloc(&tc_scratch, assign_tc_scratch_bytes(R, d)));
+    KNN_TRY(launch_assign_tc(rows, n, dp4s, d, cs->reps, R, tc_scratch, cl, dr, err, s));
+  } else {
+    KNN_TRY(launch_assign(rows, n, dp4s, cs->reps, R, cl, dr, s));
+  }
   uint64_t *keys;
   int32_t *vals;
   KNN_TRY(ar.alloc(&keys, (size_t)n));
@@ -231,7 +239,7 @@ int check_options(const knn_options *opt, knn_options *o) {
     set_error("margin must be in [0, 4096]");
     return KNN_EINVAL;
   }
-  if ((o->flags & ~KNN_SQUARED_DIST) != 0) {
+  if ((o->flags & ~(KNN_SQUARED_DIST | KNN_NO_TENSOR_CORES)) != 0) {
     set_error("unknown flags 0x%x", o->flags);
     return KNN_EINVAL;
   }
@@ -330,10 +338,18 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
     *outp = p;
     return KNN_OK;
   };
+  // [0] work counter, [1..5] statistics, [6] device error flag
+  unsigned long long *ctr;
+  KNN_TRY(ar.alloc(&ctr, 7));
+  KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, 7 * sizeof(unsigned long long), s));
+  int *dev_err = reinterpret_cast<int *>(ctr + 6);
+  const bool use_tc = (o.flags & KNN_NO_TENSOR_CORES) == 0;
+
   const float4 *Rp = nullptr, *Qp = nullptr;
   KNN_TRY(packed(r, n, &Rp));
   ClusterSet sset, qset;
-  KNN_TRY(build_clusters(ar, Rp, n, dp4s, Rs, o.seed, o.rep_trials, s, &sset));
+  KNN_TRY(build_clusters(ar, Rp, n, d, dp4s, Rs, o.seed, o.rep_trials, use_tc, dev_err, s,
+                         &sset));
   float4 *srows;
   float *sdist, *cmin, *cmax;
   int32_t *sidx;
@@ -353,7 +369,8 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
     qset = sset;
   } else {
     KNN_TRY(packed(q, m, &Qp));
-    KNN_TRY(build_clusters(ar, Qp, m, dp4s, Rq, o.seed, o.rep_trials, s, &qset));
+    KNN_TRY(build_clusters(ar, Qp, m, d, dp4s, Rq, o.seed, o.rep_trials, use_tc, dev_err, s,
+                           &qset));
   }
   float *qrad, *drr, *theta0;
   int32_t *slot_cl, *rlist, *rlen;
@@ -369,9 +386,6 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
                                k, d, theta0, rlist, rlen, s));
   KNN_TRY(evs.record(1, s));
 
-  unsigned long long *ctr;
-  KNN_TRY(ar.alloc(&ctr, 6));
-  KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, 6 * sizeof(unsigned long long), s));
   ScanArgs a{};
   a.qrows = Qp;
   a.qorder = qset.perm;
@@ -402,9 +416,13 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
   KNN_TRY(evs.record(2, s));
 
   if (st) {
-    unsigned long long h[6];
+    unsigned long long h[7];
     KNN_CUDA_TRY(cudaMemcpyAsync(h, ctr, sizeof h, cudaMemcpyDeviceToHost, s));
     KNN_CUDA_TRY(cudaStreamSynchronize(s));
+    if (static_cast<int>(h[6] & 0xffffffffu) != 0) {
+      set_error("a bounded device wait gave up (tensor-core pipeline)");
+      return KNN_ETIMEOUT;
+    }
     st->dist_evals = (int64_t)h[1];
     st->clusters_visited = (int64_t)h[2];
     st->clusters_pruned = (int64_t)h[3];
@@ -494,8 +512,11 @@ int knn_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d,
       set_error("host-to-device copy failed: %s", cudaGetErrorString(e));
       rc = KNN_ECUDA;
     }
-    if (rc == KNN_OK)
-      rc = join_device_impl(dq, m, dr, n, d, k, di, dd, opt, st, s);
+    if (rc == KNN_OK) {
+      // always the synchronising path, which also checks the device error flag
+      knn_stats local;
+      rc = join_device_impl(dq, m, dr, n, d, k, di, dd, opt, st ? st : &local, s);
+    }
     if (rc == KNN_OK) {
       e = cudaMemcpyAsync(out_idx, di, sizeof(int32_t) * m * k,
                           cudaMemcpyDeviceToHost, s);

@@ -38,6 +38,11 @@ int launch_rep_select(const float4 *rows, int dp4, const int32_t *cand_dev,
                       int32_t *rep_rows, cudaStream_t s);
 int launch_assign(const float4 *rows, int64_t n, int dp4, const float4 *reps,
                   int R, int32_t *cl, float *dr, cudaStream_t s);
+// Tensor-core assignment (assign_tc.cu): rows of d >= 16 floats.
+bool assign_tc_supported(int d);
+size_t assign_tc_scratch_bytes(int R, int d);
+int launch_assign_tc(const float4 *rows, int64_t n, int dp4, int d, const float4 *reps, int R,
+                     void *scratch, int32_t *cl, float *dr, int *err, cudaStream_t s);
 size_t cluster_sort_temp_bytes(int64_t n, int R);
 int launch_cluster_sort(const int32_t *cl, const float *dr, int64_t n, int R,
                         uint64_t *keys, int32_t *vals, uint64_t *skeys,

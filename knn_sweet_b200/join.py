@@ -43,10 +43,12 @@ class JoinStats:
 
 
 def _options(qreps, sreps, seed, rep_trials, precision, margin,
-             squared=False) -> _lib.KnnOptions:
+             squared=False, tensor_cores=True) -> _lib.KnnOptions:
     o = _lib.default_options()
     if squared:
         o.flags |= _lib.KNN_SQUARED_DIST
+    if not tensor_cores:
+        o.flags |= _lib.KNN_NO_TENSOR_CORES
     o.qreps = int(qreps)
     o.sreps = int(sreps)
     o.seed = int(seed) & 0xFFFFFFFF
@@ -68,7 +70,8 @@ def _is_torch(x) -> bool:
 
 def knnjoin(queries, sources=None, k: int = 200, *, qreps: int = 0, sreps: int = 0,
             seed: int = 2015, rep_trials: int = 10, precision: str = "fp32",
-            margin: int = 32, stats: bool = False, out=None, squared: bool = False):
+            margin: int = 32, stats: bool = False, out=None, squared: bool = False,
+            tensor_cores: bool = True):
     """Exact k nearest neighbours of every query row among the source rows.
 
     queries: (m, d) float32; sources: (n, d) float32 or None for a self-join
@@ -77,10 +80,11 @@ def knnjoin(queries, sources=None, k: int = 200, *, qreps: int = 0, sreps: int =
     ties to the lower source row; slots beyond n hold (-1, inf).  With
     stats=True a JoinStats is returned as a third element.  `out` may give
     preallocated (idx, dist) arrays of the input's kind (e.g. pinned host
-    memory for the host path).  squared=True returns squared distances.
+    memory for the host path).  squared=True returns squared distances;
+    tensor_cores=False keeps every stage on CUDA-core FP32 kernels.
     """
     lib = _lib.load()
-    opt = _options(qreps, sreps, seed, rep_trials, precision, margin, squared)
+    opt = _options(qreps, sreps, seed, rep_trials, precision, margin, squared, tensor_cores)
     st = _lib.KnnStats()
     stp = ctypes.byref(st) if stats else None
     if _is_torch(queries) and queries.is_cuda:

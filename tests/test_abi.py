@@ -84,7 +84,7 @@ def test_bad_sizes_are_rejected(d, k):
 
 def test_bad_options_are_rejected():
     x = np.zeros((4, 3), np.float32)
-    for field, val in [("flags", 2), ("qreps", -1), ("sreps", 9000), ("rep_trials", 0),
+    for field, val in [("flags", 4), ("flags", 0x100), ("qreps", -1), ("sreps", 9000), ("rep_trials", 0),
                        ("precision", 7), ("margin", -2)]:
         o = _lib.default_options()
         setattr(o, field, val)
