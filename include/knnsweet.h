@@ -75,6 +75,11 @@ typedef struct knn_options {
   int32_t margin;     /* extra candidates re-ranked by the BF16 form         */
   int32_t autotune;   /* batched form: pick tiles per cloud-size bucket      */
   int32_t flags;      /* KNN_SQUARED_DIST | KNN_NO_TENSOR_CORES, or 0        */
+  int32_t lloyd_iters;/* representative refinement: after the draw, this many
+                         steps of "move every representative to its cluster's
+                         centroid, re-assign" (0 = the reference's draw only;
+                         default 0)                                          */
+  int32_t reserved0;
 } knn_options;
 
 /*

@@ -38,6 +38,8 @@ class KnnOptions(ctypes.Structure):
         ("margin", ctypes.c_int32),
         ("autotune", ctypes.c_int32),
         ("flags", ctypes.c_int32),
+        ("lloyd_iters", ctypes.c_int32),
+        ("reserved0", ctypes.c_int32),
     ]
 
 

@@ -175,8 +175,8 @@ struct ClusterSet {
 };
 
 int build_clusters(Arena &ar, const float4 *rows, int64_t n, int d, int dp4s, int R,
-                   uint32_t seed, int trials, bool use_tc, int *err, cudaStream_t s,
-                   ClusterSet *cs) {
+                   uint32_t seed, int trials, int lloyd_iters, bool use_tc, int *err,
+                   cudaStream_t s, ClusterSet *cs) {
   cs->R = R;
   // representative draw on the host: trials x R indices rand() % n
   std::vector<int32_t> cand((size_t)trials * R);
@@ -195,14 +195,9 @@ int build_clusters(Arena &ar, const float4 *rows, int64_t n, int d, int dp4s, in
   float *dr;
   KNN_TRY(ar.alloc(&cl, (size_t)n));
   KNN_TRY(ar.alloc(&dr, (size_t)n));
-  if (use_tc && assign_tc_supported(d)) {
-    // BF16 tensor-core arg-min, then the exact FP32 distance to the winner
-    unsigned char *tc_scratch;
-    KNN_TRY(ar.alloc(&tc_scratch, assign_tc_scratch_bytes(R, d)));
-    KNN_TRY(launch_assign_tc(rows, n, dp4s, d, cs->reps, R, tc_scratch, cl, dr, err, s));
-  } else {
-    KNN_TRY(launch_assign(rows, n, dp4s, cs->reps, R, cl, dr, s));
-  }
+  const bool tc_assign = use_tc && assign_tc_supported(d);
+  unsigned char *tc_scratch = nullptr;
+  if (tc_assign) KNN_TRY(ar.alloc(&tc_scratch, assign_tc_scratch_bytes(R, d)));
   uint64_t *keys;
   int32_t *vals;
   KNN_TRY(ar.alloc(&keys, (size_t)n));
@@ -212,10 +207,21 @@ int build_clusters(Arena &ar, const float4 *rows, int64_t n, int d, int dp4s, in
   size_t temp_bytes = cluster_sort_temp_bytes(n, R);
   unsigned char *temp;
   KNN_TRY(ar.alloc(&temp, temp_bytes));
-  KNN_TRY(launch_cluster_sort(cl, dr, n, R, keys, vals, cs->skeys, cs->perm, temp,
-                              temp_bytes, s));
   KNN_TRY(ar.alloc(&cs->off, (size_t)R + 1));
-  KNN_TRY(launch_cluster_offsets(cs->skeys, n, R, cs->off, s));
+  // nearest representative (BF16 tensor-core arg-min + exact FP32 distance to
+  // the winner for d >= 16, FP32 CUDA cores otherwise), then one sort into
+  // clusters; with Lloyd steps the representatives move to their clusters'
+  // centroids and the points are assigned and sorted again
+  for (int it = 0; it <= lloyd_iters; it++) {
+    if (it > 0) KNN_TRY(launch_centroids(rows, dp4s, cs->perm, cs->off, R, cs->reps, s));
+    if (tc_assign)
+      KNN_TRY(launch_assign_tc(rows, n, dp4s, d, cs->reps, R, tc_scratch, cl, dr, err, s));
+    else
+      KNN_TRY(launch_assign(rows, n, dp4s, cs->reps, R, cl, dr, s));
+    KNN_TRY(launch_cluster_sort(cl, dr, n, R, keys, vals, cs->skeys, cs->perm, temp,
+                                temp_bytes, s));
+    KNN_TRY(launch_cluster_offsets(cs->skeys, n, R, cs->off, s));
+  }
   return KNN_OK;
 }
 
@@ -237,6 +243,10 @@ int check_options(const knn_options *opt, knn_options *o) {
   }
   if (o->margin < 0 || o->margin > 4096) {
     set_error("margin must be in [0, 4096]");
+    return KNN_EINVAL;
+  }
+  if (o->lloyd_iters < 0 || o->lloyd_iters > 100) {
+    set_error("lloyd_iters must be in [0, 100]");
     return KNN_EINVAL;
   }
   if ((o->flags & ~(KNN_SQUARED_DIST | KNN_NO_TENSOR_CORES)) != 0) {
@@ -348,7 +358,7 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
   const float4 *Rp = nullptr, *Qp = nullptr;
   KNN_TRY(packed(r, n, &Rp));
   ClusterSet sset, qset;
-  KNN_TRY(build_clusters(ar, Rp, n, d, dp4s, Rs, o.seed, o.rep_trials, use_tc, dev_err, s,
+  KNN_TRY(build_clusters(ar, Rp, n, d, dp4s, Rs, o.seed, o.rep_trials, o.lloyd_iters, use_tc, dev_err, s,
                          &sset));
   float4 *srows;
   float *sdist, *cmin, *cmax;
@@ -369,7 +379,7 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
     qset = sset;
   } else {
     KNN_TRY(packed(q, m, &Qp));
-    KNN_TRY(build_clusters(ar, Qp, m, d, dp4s, Rq, o.seed, o.rep_trials, use_tc, dev_err, s,
+    KNN_TRY(build_clusters(ar, Qp, m, d, dp4s, Rq, o.seed, o.rep_trials, o.lloyd_iters, use_tc, dev_err, s,
                            &qset));
   }
   float *qrad, *drr, *theta0;

@@ -171,6 +171,54 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Lloyd step: every representative moves to the centroid of its members.
+// One block per cluster; members are read in cluster order (perm) and summed
+// with a fixed assignment of members to threads and a fixed tree, so the
+// result does not depend on scheduling.  Empty clusters keep their
+// representative.  (Representative refinement is not in the reference, which
+// keeps the best of its random draws, knnjoin.cu:125-154.)
+__global__ void __launch_bounds__(256)
+    centroid_kernel(const float4 *__restrict__ rows, int dp4, const int32_t *__restrict__ perm,
+                    const int32_t *__restrict__ off, float4 *__restrict__ reps) {
+  __shared__ float4 red[256];
+  const int c = blockIdx.x, tid = threadIdx.x;
+  const int a = off[c], b = off[c + 1];
+  if (b == a) return;
+  const float inv = 1.0f / (float)(b - a);
+  for (int ch = 0; ch < dp4; ch++) {
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int p = a + tid; p < b; p += 256) {
+      const float4 v = rows[(int64_t)perm[p] * dp4 + ch];
+      acc.x += v.x;
+      acc.y += v.y;
+      acc.z += v.z;
+      acc.w += v.w;
+    }
+    red[tid] = acc;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+      if (tid < s) {
+        red[tid].x += red[tid + s].x;
+        red[tid].y += red[tid + s].y;
+        red[tid].z += red[tid + s].z;
+        red[tid].w += red[tid + s].w;
+      }
+      __syncthreads();
+    }
+    if (tid == 0)
+      reps[(int64_t)c * dp4 + ch] =
+          make_float4(red[0].x * inv, red[0].y * inv, red[0].z * inv, red[0].w * inv);
+    __syncthreads();
+  }
+}
+
+int launch_centroids(const float4 *rows, int dp4, const int32_t *perm, const int32_t *off, int R,
+                     float4 *reps, cudaStream_t s) {
+  centroid_kernel<<<R, 256, 0, s>>>(rows, dp4, perm, off, reps);
+  KNN_LAUNCH_CHECK();
+  return KNN_OK;
+}
+
 // Sort keys (cluster << 32 | distance bits) and identity values.
 __global__ void cluster_keys_kernel(const int32_t *__restrict__ cl,
                                     const float *__restrict__ dr, int64_t n,

@@ -43,8 +43,9 @@ class JoinStats:
 
 
 def _options(qreps, sreps, seed, rep_trials, precision, margin,
-             squared=False, tensor_cores=True) -> _lib.KnnOptions:
+             squared=False, tensor_cores=True, lloyd_iters=0) -> _lib.KnnOptions:
     o = _lib.default_options()
+    o.lloyd_iters = int(lloyd_iters)
     if squared:
         o.flags |= _lib.KNN_SQUARED_DIST
     if not tensor_cores:
@@ -71,7 +72,7 @@ def _is_torch(x) -> bool:
 def knnjoin(queries, sources=None, k: int = 200, *, qreps: int = 0, sreps: int = 0,
             seed: int = 2015, rep_trials: int = 10, precision: str = "fp32",
             margin: int = 32, stats: bool = False, out=None, squared: bool = False,
-            tensor_cores: bool = True):
+            tensor_cores: bool = True, lloyd_iters: int = 0):
     """Exact k nearest neighbours of every query row among the source rows.
 
     queries: (m, d) float32; sources: (n, d) float32 or None for a self-join
@@ -81,10 +82,12 @@ def knnjoin(queries, sources=None, k: int = 200, *, qreps: int = 0, sreps: int =
     stats=True a JoinStats is returned as a third element.  `out` may give
     preallocated (idx, dist) arrays of the input's kind (e.g. pinned host
     memory for the host path).  squared=True returns squared distances;
-    tensor_cores=False keeps every stage on CUDA-core FP32 kernels.
+    tensor_cores=False keeps every stage on CUDA-core FP32 kernels;
+    lloyd_iters > 0 refines the representatives (centroid steps).
     """
     lib = _lib.load()
-    opt = _options(qreps, sreps, seed, rep_trials, precision, margin, squared, tensor_cores)
+    opt = _options(qreps, sreps, seed, rep_trials, precision, margin, squared, tensor_cores,
+                   lloyd_iters)
     st = _lib.KnnStats()
     stp = ctypes.byref(st) if stats else None
     if _is_torch(queries) and queries.is_cuda:

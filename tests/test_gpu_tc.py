@@ -68,3 +68,14 @@ def test_join_identical_with_and_without_tensor_cores(cuda_device, d, k):
     a = knnjoin(q, r, k, qreps=150, sreps=150)
     b = knnjoin(q, r, k, qreps=150, sreps=150, tensor_cores=False)
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+@pytest.mark.parametrize("d,k,iters", [(3, 50, 2), (32, 16, 3)])
+def test_lloyd_refinement_keeps_results(cuda_device, oracle, d, k, iters):
+    r, q = data.gaussian_mix(25000, 1500, d, 80, seed=600 + d)
+    idx, dist, st = knnjoin(q, r, k, qreps=120, sreps=120, lloyd_iters=iters, stats=True)
+    oi, od = oracle.bruteforce_f64(q, r, k)
+    assert (idx == oi).all(axis=1).mean() > 0.999
+    np.testing.assert_allclose(dist, od, rtol=1e-5)
+    b = knnjoin(q, r, k, qreps=120, sreps=120, lloyd_iters=iters)
+    assert np.array_equal(idx, b[0]) and np.array_equal(dist, b[1])  # deterministic
