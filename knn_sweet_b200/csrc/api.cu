@@ -575,3 +575,41 @@ void knn_pack_indexdist(const int32_t *idx, const float *dist, int64_t count,
 }
 
 }  // extern "C"
+
+// Test hook (not part of the public ABI): the representative rows the
+// seeded draw picks (the reference's 10-trial spread selection,
+// src/knnjoin.cu:195-239, 125-154) for device points pts (n x d floats);
+// rows_out is a device array of R ints.
+extern "C" int knnsweet_test_select_reps(const float *pts, int64_t n, int32_t d, int32_t R,
+                                         uint32_t seed, int32_t trials, int32_t *rows_out) {
+  using namespace knnsweet;
+  error_buffer().clear();
+  if (!pts || !rows_out || n <= 0 || d <= 0 || R <= 0 || R > n || trials <= 0) {
+    set_error("bad arguments");
+    return KNN_EINVAL;
+  }
+  cudaStream_t s = 0;
+  int rc = KNN_OK;
+  {
+    Arena ar(s);
+    const int dp4 = (d + 3) / 4;
+    float4 *rows = nullptr, *reps = nullptr;
+    int32_t *cand = nullptr;
+    uint32_t *score = nullptr;
+    std::vector<int32_t> draw((size_t)trials * R);
+    GlibcRand g(seed);
+    for (auto &c : draw) c = g.next() % (int32_t)n;
+    rc = ar.alloc(&rows, (size_t)n * dp4);
+    if (rc == KNN_OK) rc = ar.alloc(&reps, (size_t)R * dp4);
+    if (rc == KNN_OK) rc = ar.alloc(&cand, draw.size());
+    if (rc == KNN_OK) rc = ar.alloc(&score, (size_t)trials);
+    if (rc == KNN_OK) rc = launch_pack_rows(pts, n, d, dp4, rows, s);
+    if (rc == KNN_OK) rc = upload_i32(draw, cand, s);
+    if (rc == KNN_OK) rc = launch_rep_select(rows, dp4, cand, R, trials, score, reps, rows_out, s);
+  }
+  if (rc == KNN_OK && cudaStreamSynchronize(s) != cudaSuccess) {
+    set_error("device failure");
+    rc = KNN_ECUDA;
+  }
+  return rc;
+}

@@ -43,26 +43,73 @@ __global__ void pack_rows_kernel(const float *__restrict__ src, int64_t n,
 // Representative draw (src/knnjoin.cu:125-154, host draw 195-239).
 // cand[t * R + i] are row indices drawn on the host with the glibc generator.
 // score[t] = wrapping int32 sum over ordered pairs (i, j) of (int)dist.
-// grid: (ceil(R / blockDim), trials)
+// Tiled: a block owns 64 x 64 candidate pairs of one trial; rows are staged
+// through shared memory 32 floats at a time and every thread accumulates 16
+// pairs (i = i0 + ty + 16a, j = j0 + tx + 16b), each summed in dimension
+// order with fma, exactly as the one-pair distance would be.
+// grid: (ceil(R / 64), ceil(R / 64), trials), 256 threads
 // ---------------------------------------------------------------------------
-__global__ void rep_score_kernel(const float4 *__restrict__ rows, int dp4,
-                                 const int32_t *__restrict__ cand, int R,
-                                 uint32_t *__restrict__ score) {
-  int t = blockIdx.y;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256)
+    rep_score_kernel(const float4 *__restrict__ rows, int dp4,
+                     const int32_t *__restrict__ cand, int R,
+                     uint32_t *__restrict__ score) {
+  __shared__ float4 sa[8][64];
+  __shared__ float4 sb[8][64];
+  __shared__ uint32_t red[8];
+  const int t = blockIdx.z;
+  const int i0 = blockIdx.x * 64, j0 = blockIdx.y * 64;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int32_t *c = cand + (int64_t)t * R;
-  uint32_t sum = 0;
-  if (i < R) {
-    const float4 *a = rows + (int64_t)c[i] * dp4;
-    for (int j = 0; j < R; j++) {
-      const float4 *b = rows + (int64_t)c[j] * dp4;
-      float dd = sqrtf(dist2_rows_rt(a, b, dp4));
-      sum += (uint32_t)(int32_t)dd;
+  float acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[a][b] = 0.0f;
+  for (int ch = 0; ch < dp4; ch += 8) {
+    const int nch = min(8, dp4 - ch);
+    for (int e = threadIdx.x; e < 64 * 8; e += 256) {
+      const int r = e & 63, q = e >> 6;
+      const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+      sa[q][r] = (q < nch && i0 + r < R) ? rows[(int64_t)c[i0 + r] * dp4 + ch + q] : zero;
+      sb[q][r] = (q < nch && j0 + r < R) ? rows[(int64_t)c[j0 + r] * dp4 + ch + q] : zero;
     }
+    __syncthreads();
+    for (int q = 0; q < nch; q++) {
+      float4 av[4], bv[4];
+#pragma unroll
+      for (int a = 0; a < 4; a++) av[a] = sa[q][ty + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; b++) bv[b] = sb[q][tx + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+          float s = acc[a][b], u;
+          u = __fsub_rn(av[a].x, bv[b].x); s = __fmaf_rn(u, u, s);
+          u = __fsub_rn(av[a].y, bv[b].y); s = __fmaf_rn(u, u, s);
+          u = __fsub_rn(av[a].z, bv[b].z); s = __fmaf_rn(u, u, s);
+          u = __fsub_rn(av[a].w, bv[b].w); s = __fmaf_rn(u, u, s);
+          acc[a][b] = s;
+        }
+    }
+    __syncthreads();
   }
-  // warp reduce then one atomic per warp (wrapping unsigned add)
+  uint32_t sum = 0;
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+      if (i0 + ty + 16 * a < R && j0 + tx + 16 * b < R)
+        sum += (uint32_t)(int32_t)sqrtf(acc[a][b]);
+  // block reduce (wrapping unsigned add), one atomic per block
   for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(score + t, sum);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t tot = 0;
+    for (int w = 0; w < 8; w++) tot += red[w];
+    atomicAdd(score + t, tot);
+  }
 }
 
 // Picks the first trial whose score, compared as float against a running
@@ -367,20 +414,41 @@ __global__ void __launch_bounds__(512)
   const int64_t n = soff[Rs];
   const int kk = (int)(k < n ? k : n);
 
-  // upper end of the bisection: the largest value any cluster contributes
-  unsigned hi_local = 0;
+  // upper end of the bisection: the largest value any cluster contributes,
+  // or better, the kk-th value of any single cluster holding kk members
+  // (that cluster alone has kk values at or below it).  Each cluster's
+  // smallest value is kept in shared memory (the sort keys' space, reused
+  // below): a cluster whose smallest value exceeds T adds nothing to the
+  // count at T and skips its search.
+  float *lo_v = reinterpret_cast<float *>(skey);
+  unsigned hi_local = 0, u_local = 0xffffffffu;
   for (int j = tid; j < Rs; j += nth) {
     int a = soff[j], sz = min(soff[j + 1] - a, kk);
+    float first = __int_as_float(0x7f800000);
     if (sz > 0) {
-      float v = __fadd_rn(__fadd_rn(rq, dq[j]), sdist[a + sz - 1]);
+      const float base = __fadd_rn(rq, dq[j]);
+      float v = __fadd_rn(base, sdist[a + sz - 1]);
       hi_local = max(hi_local, __float_as_uint(v));
+      if (sz == kk) u_local = min(u_local, __float_as_uint(v));
+      first = __fadd_rn(base, sdist[a]);
     }
+    lo_v[j] = first;
   }
-  for (int o = 16; o > 0; o >>= 1) hi_local = max(hi_local, __shfl_xor_sync(kFull, hi_local, o));
-  if (lane == 0) red_u[warp] = hi_local;
+  for (int o = 16; o > 0; o >>= 1) {
+    hi_local = max(hi_local, __shfl_xor_sync(kFull, hi_local, o));
+    u_local = min(u_local, __shfl_xor_sync(kFull, u_local, o));
+  }
+  if (lane == 0) {
+    red_u[warp] = hi_local;
+    red_i[warp] = (int)u_local;
+  }
   __syncthreads();
-  unsigned hi = 0;
-  for (int w = 0; w < nwarp; w++) hi = max(hi, red_u[w]);
+  unsigned hi = 0, u = 0xffffffffu;
+  for (int w = 0; w < nwarp; w++) {
+    hi = max(hi, red_u[w]);
+    u = min(u, (unsigned)red_i[w]);
+  }
+  if (u < hi) hi = u;
   __syncthreads();
   // smallest bit pattern T with count(values <= T) >= kk; count(hi) >= kk.
   unsigned lo = 0;  // count(lo - 1) < kk is implied for lo = 0
@@ -390,8 +458,8 @@ __global__ void __launch_bounds__(512)
     float T = __uint_as_float(mid);
     int cnt = 0;
     for (int j = tid; j < Rs; j += nth) {
+      if (lo_v[j] > T) continue;  // empty cluster (+inf) or nothing <= T
       int a = soff[j], sz = min(soff[j + 1] - a, kk);
-      if (sz == 0) continue;
       float base = __fadd_rn(rq, dq[j]);
       int l = 0, h = sz;  // first t with base + sdist[a+t] > T
       while (l < h) {
@@ -475,8 +543,8 @@ int launch_rep_select(const float4 *rows, int dp4, const int32_t *cand_dev,
                       int R, int trials, uint32_t *score_dev, float4 *reps,
                       int32_t *rep_rows, cudaStream_t s) {
   KNN_CUDA_TRY(cudaMemsetAsync(score_dev, 0, sizeof(uint32_t) * trials, s));
-  dim3 grid((R + 127) / 128, trials);
-  rep_score_kernel<<<grid, 128, 0, s>>>(rows, dp4, cand_dev, R, score_dev);
+  dim3 grid((R + 63) / 64, (R + 63) / 64, trials);
+  rep_score_kernel<<<grid, 256, 0, s>>>(rows, dp4, cand_dev, R, score_dev);
   KNN_LAUNCH_CHECK();
   rep_pick_kernel<<<1, 256, 0, s>>>(rows, dp4, cand_dev, R, trials, score_dev,
                                     reps, rep_rows);

@@ -79,3 +79,24 @@ def test_lloyd_refinement_keeps_results(cuda_device, oracle, d, k, iters):
     np.testing.assert_allclose(dist, od, rtol=1e-5)
     b = knnjoin(q, r, k, qreps=120, sreps=120, lloyd_iters=iters)
     assert np.array_equal(idx, b[0]) and np.array_equal(dist, b[1])  # deterministic
+
+
+@pytest.mark.parametrize("n,d,R", [(5000, 3, 100), (20000, 3, 800), (8000, 32, 300), (3000, 128, 200)])
+def test_representative_draw_matches_reference_procedure(cuda_device, oracle, n, d, R):
+    """The GPU draw (10 seeded trials scored by pairwise spread) picks the same
+    rows as the reference's procedure restated in the oracle."""
+    import torch
+    if d == 3:
+        pts = data.skin_like(n, seed=70 + R)
+    else:
+        pts = data.gaussian_mix(n, 1, d, 30, seed=71 + d)[0]
+    lib = _lib.load()
+    fn = lib.knnsweet_test_select_reps
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
+                   ctypes.c_uint32, ctypes.c_int32, ctypes.c_void_p]
+    p = torch.from_numpy(pts).cuda()
+    out = torch.full((R,), -1, dtype=torch.int32, device="cuda")
+    assert fn(p.data_ptr(), n, d, R, 2015, 10, out.data_ptr()) == 0, lib.knn_last_error()
+    want, _ = oracle.select_reps(pts, R, seed=2015, trials=10)
+    assert np.array_equal(out.cpu().numpy(), want)
