@@ -181,6 +181,35 @@ int knn_join_device_noalloc(const float *q, int64_t m, const float *r, int64_t n
                             void *stream);
 
 /*
+ * Batched join: `ncloud` independent joins in one call (no reference
+ * counterpart as an entry point; per cloud it computes what one reference
+ * run, src/knnjoin.cu:983-1145, computes for one pair of point sets).
+ * Cloud c's queries are rows q_offsets[c] .. q_offsets[c+1]-1 of q and its
+ * reference points rows r_offsets[c] .. r_offsets[c+1]-1 of r; every query
+ * gets its k nearest among its own cloud's reference points only, and
+ * out_idx holds indices RELATIVE to r_offsets[c] (0-based within the cloud),
+ * rows in q's order, -1 / +inf where the cloud has fewer than k points.
+ *  - q, r, out_idx, out_dist: device memory; q_offsets, r_offsets: HOST
+ *    arrays of ncloud + 1 non-decreasing int64 starting at 0.
+ *  - Passing q == r and equal offsets makes it a per-cloud self-join.
+ *  - 1 <= d <= 32, 1 <= k <= 256.  qreps / sreps / lloyd_iters / margin are
+ *    ignored: each cloud of n points gets about alpha * sqrt(n)
+ *    representatives (at most 2048), alpha chosen per cloud-size bucket
+ *    (powers of two) by timing when opt->autotune is set (the first call per
+ *    (d, k, bucket) synchronises the stream; the choice is cached for the
+ *    process), 1.6 otherwise.  Representative draws use a counter-based
+ *    hash of (seed, cloud, trial, slot), best of rep_trials by spread.
+ *  - Once tuned, the call enqueues without host synchronisation (unless `st`
+ *    is given) and its scratch comes from the library's stream-ordered pool.
+ */
+int knn_join_batched_device(const float *q, const int64_t *q_offsets,
+                            const float *r, const int64_t *r_offsets,
+                            int32_t ncloud, int32_t d, int32_t k,
+                            int32_t *out_idx, float *out_dist,
+                            const knn_options *opt, knn_stats *st,
+                            void *stream);
+
+/*
  * Returns the device scratch memory the library keeps cached between calls
  * (one stream-ordered pool per device; no reference counterpart: the
  * reference never frees its device memory).  Memory still in use by calls in

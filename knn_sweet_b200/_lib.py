@@ -80,6 +80,9 @@ SIGNATURES = {
     "knn_trim_memory": (_c_int, []),
     "knn_join_device_noalloc": (_c_int, [_vp, _c_i64, _vp, _c_i64, _c_i32, _c_i32, _vp, _vp,
                                          ctypes.POINTER(KnnOptions), _vp]),
+    "knn_join_batched_device": (_c_int, [_vp, _vp, _vp, _vp, _c_i32, _c_i32, _c_i32, _vp, _vp,
+                                         ctypes.POINTER(KnnOptions),
+                                         ctypes.POINTER(KnnStats), _vp]),
 }
 
 _lock = threading.Lock()

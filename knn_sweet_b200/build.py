@@ -32,8 +32,8 @@ NVCC_FLAGS = ARCH + [
     "-Xcompiler", "-Wall", "-I", str(ROOT / "include"),
 ]
 
-CU_SOURCES = ["api.cu", "build_index.cu", "scan.cu", "backward.cu", "noalloc.cu", "assign_tc.cu"]
-HEADERS = ["common.cuh", "kernels.cuh", "glibc_rand.h", "tc_common.cuh"]
+CU_SOURCES = ["api.cu", "build_index.cu", "scan.cu", "backward.cu", "noalloc.cu", "assign_tc.cu", "batched.cu"]
+HEADERS = ["common.cuh", "kernels.cuh", "glibc_rand.h", "tc_common.cuh", "bounds.cuh"]
 
 
 def nvcc() -> str:

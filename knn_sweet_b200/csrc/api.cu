@@ -45,8 +45,6 @@ void set_error(const char *fmt, ...) {
   error_buffer() = buf;
 }
 
-namespace {
-
 // One stream-ordered memory pool per device for the library's scratch.  Its
 // release threshold is unlimited, so memory freed at the end of a call stays
 // cached for the next call instead of going back to the driver at every
@@ -78,6 +76,8 @@ int scratch_pool(cudaMemPool_t *out) {
   *out = g_pools[dev];
   return KNN_OK;
 }
+
+namespace {
 
 // Stream-ordered scratch: every allocation is released on the same stream
 // when the arena goes out of scope.

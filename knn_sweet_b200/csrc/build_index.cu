@@ -13,6 +13,7 @@
 //                          reference clusters sorted by rep-rep distance
 #include <cub/device/device_radix_sort.cuh>
 
+#include "bounds.cuh"
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -368,22 +369,7 @@ __global__ void rep_dist_kernel(const float4 *__restrict__ qreps, int Rq,
   }
 }
 
-// ---------------------------------------------------------------------------
-// Per query cluster (one block each):
-//  1. theta0 = k-th smallest over all reference points s of
-//     rq + d(Rq, Rs(s)) + d(s, Rs(s)), the bound RepsUpperBound computes
-//     (knnjoin.cu:459-504), found exactly by bisection on the value's bit
-//     pattern with a count of values <= T (binary search per cluster over its
-//     first min(k, size) members).  The reference keeps the K smallest in a
-//     list and replaces every entry equal to the maximum at once (486-489,
-//     defect B2), which undercounts ties; the count here is exact.  Widened
-//     by the rounding slack.
-//  2. The reference clusters Rs that can hold a point within theta0 of some
-//     query of the cluster: d(Rq,Rs) - rq - radius(Rs) <= theta0
-//     (FilterReps, knnjoin.cu:506-525), sorted by d(Rq,Rs), then Rs
-//     (the host std::sort of knnjoin.cu:1080-1091).
 // dynamic shared memory: RsPow2 * 8 bytes (sort keys).
-// ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(512)
     bounds_filter_kernel(const float *__restrict__ drr, int Rq, int Rs,
                          const float *__restrict__ qrad,
@@ -395,130 +381,16 @@ __global__ void __launch_bounds__(512)
                          int32_t *__restrict__ rlist,
                          int32_t *__restrict__ rlen) {
   extern __shared__ uint64_t skey[];
-  __shared__ int red_i[32];
-  __shared__ unsigned red_u[32];
-  __shared__ int kept_s;
   const int qc = blockIdx.x;
-  const int tid = threadIdx.x, nth = blockDim.x;
-  const int lane = tid & 31, warp = tid >> 5, nwarp = nth >> 5;
-  const float tol = bound_tol(d);
   if (qoff[qc + 1] == qoff[qc]) {  // empty query cluster
-    if (tid == 0) {
+    if (threadIdx.x == 0) {
       theta0[qc] = 0.0f;
       rlen[qc] = 0;
     }
     return;
   }
-  const float rq = qrad[qc];
-  const float *dq = drr + (int64_t)qc * Rs;
-  const int64_t n = soff[Rs];
-  const int kk = (int)(k < n ? k : n);
-
-  // upper end of the bisection: the largest value any cluster contributes,
-  // or better, the kk-th value of any single cluster holding kk members
-  // (that cluster alone has kk values at or below it).  Each cluster's
-  // smallest value is kept in shared memory (the sort keys' space, reused
-  // below): a cluster whose smallest value exceeds T adds nothing to the
-  // count at T and skips its search.
-  float *lo_v = reinterpret_cast<float *>(skey);
-  unsigned hi_local = 0, u_local = 0xffffffffu;
-  for (int j = tid; j < Rs; j += nth) {
-    int a = soff[j], sz = min(soff[j + 1] - a, kk);
-    float first = __int_as_float(0x7f800000);
-    if (sz > 0) {
-      const float base = __fadd_rn(rq, dq[j]);
-      float v = __fadd_rn(base, sdist[a + sz - 1]);
-      hi_local = max(hi_local, __float_as_uint(v));
-      if (sz == kk) u_local = min(u_local, __float_as_uint(v));
-      first = __fadd_rn(base, sdist[a]);
-    }
-    lo_v[j] = first;
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    hi_local = max(hi_local, __shfl_xor_sync(kFull, hi_local, o));
-    u_local = min(u_local, __shfl_xor_sync(kFull, u_local, o));
-  }
-  if (lane == 0) {
-    red_u[warp] = hi_local;
-    red_i[warp] = (int)u_local;
-  }
-  __syncthreads();
-  unsigned hi = 0, u = 0xffffffffu;
-  for (int w = 0; w < nwarp; w++) {
-    hi = max(hi, red_u[w]);
-    u = min(u, (unsigned)red_i[w]);
-  }
-  if (u < hi) hi = u;
-  __syncthreads();
-  // smallest bit pattern T with count(values <= T) >= kk; count(hi) >= kk.
-  unsigned lo = 0;  // count(lo - 1) < kk is implied for lo = 0
-  // invariant: answer in [lo, hi]
-  while (lo < hi) {
-    unsigned mid = lo + ((hi - lo) >> 1);
-    float T = __uint_as_float(mid);
-    int cnt = 0;
-    for (int j = tid; j < Rs; j += nth) {
-      if (lo_v[j] > T) continue;  // empty cluster (+inf) or nothing <= T
-      int a = soff[j], sz = min(soff[j + 1] - a, kk);
-      float base = __fadd_rn(rq, dq[j]);
-      int l = 0, h = sz;  // first t with base + sdist[a+t] > T
-      while (l < h) {
-        int md = (l + h) >> 1;
-        if (__fadd_rn(base, sdist[a + md]) <= T) l = md + 1;
-        else h = md;
-      }
-      cnt += l;
-    }
-    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kFull, cnt, o);
-    if (lane == 0) red_i[warp] = cnt;
-    __syncthreads();
-    int total = 0;
-    for (int w = 0; w < nwarp; w++) total += red_i[w];
-    __syncthreads();
-    if (total >= kk) hi = mid;
-    else lo = mid + 1;
-  }
-  const float kth = __uint_as_float(hi);
-  const float th = __fmaf_rn(kth, 4.0f * tol, kth) + 1.17549435e-38f;
-  if (tid == 0) {
-    theta0[qc] = th;
-    kept_s = 0;
-  }
-  __syncthreads();
-
-  // filter + sort the survivors by (d(Rq,Rs), Rs)
-  for (int j = tid; j < rs_pow2; j += nth) {
-    uint64_t key = kKeyMax;
-    if (j < Rs && soff[j + 1] > soff[j]) {
-      float dd = dq[j], rr = scmax[j];
-      float lb = dd - rq - rr;
-      if (!(lb > th + tol * (dd + rq + rr + th))) {
-        key = ((uint64_t)__float_as_uint(dd) << 32) | (uint32_t)j;
-        atomicAdd(&kept_s, 1);
-      }
-    }
-    skey[j] = key;
-  }
-  __syncthreads();
-  for (int size = 2; size <= rs_pow2; size <<= 1) {
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int t = tid; t < (rs_pow2 >> 1); t += nth) {
-        int i = 2 * t - (t & (stride - 1));
-        int j = i + stride;
-        bool up = (i & size) == 0;
-        uint64_t a = skey[i], b = skey[j];
-        if ((a > b) == up) {
-          skey[i] = b;
-          skey[j] = a;
-        }
-      }
-      __syncthreads();
-    }
-  }
-  const int kept = kept_s;
-  for (int j = tid; j < kept; j += nth)
-    rlist[(int64_t)qc * Rs + j] = (int32_t)(skey[j] & 0xffffffffu);
-  if (tid == 0) rlen[qc] = kept;
+  bounds_filter_block(drr + (int64_t)qc * Rs, Rs, soff, sdist, scmax, qrad[qc], k, d, rs_pow2,
+                      0, skey, theta0 + qc, rlist + (int64_t)qc * Rs, rlen + qc);
 }
 
 // ---------------------------------------------------------------------------

@@ -112,6 +112,8 @@ std::string &error_buffer();
 // Per-thread count of kernels enqueued by the current call (reported in
 // knn_stats.kernels_launched); every launch site ends in KNN_LAUNCH_CHECK.
 int &launch_counter();
+// The per-device stream-ordered pool the library draws its scratch from.
+int scratch_pool(cudaMemPool_t *out);
 
 }  // namespace knnsweet
 

@@ -24,6 +24,10 @@ struct ScanArgs {
   const float *theta0;      // Rq: initial k-th bound per query cluster
   const int32_t *rlist;     // Rq x Rs surviving clusters, nearest first
   const int32_t *rlen;      // Rq
+  const int64_t *rl_base;   // batched form: start of each query cluster's list
+                            // in rlist (null: qc * Rs)
+  const int64_t *qc_ref_base;  // batched form: subtracted from every output
+                               // index of query cluster qc (null: 0)
   int Rs;
   int32_t *out_idx;         // m x k
   float *out_dist;          // m x k

@@ -181,7 +181,7 @@ struct RegTopK : TopKBase {
   }
 
   // Writes the k results (through the buffer for coalesced stores).
-  __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int lane) {
+  __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int32_t base, int lane) {
     __syncwarp();
 #pragma unroll
     for (int j = 0; j < E; j++) buf[E * lane + j] = v[j];
@@ -189,7 +189,7 @@ struct RegTopK : TopKBase {
     for (int t = lane; t < k; t += 32) {
       const uint64_t key = buf[t];
       const bool none = key == kKeyMax;
-      oi[t] = none ? -1 : key_idx(key);
+      oi[t] = none ? -1 : key_idx(key) - base;
       od[t] = none ? __int_as_float(0x7f800000) : (squared ? key_d2(key) : sqrtf(key_d2(key)));
     }
     __syncwarp();
@@ -285,11 +285,11 @@ struct SmemTopK : TopKBase {
     }
   }
 
-  __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int lane) {
+  __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int32_t base, int lane) {
     for (int t = lane; t < k; t += 32) {
       const uint64_t key = list[t];
       const bool none = key == kKeyMax;
-      oi[t] = none ? -1 : key_idx(key);
+      oi[t] = none ? -1 : key_idx(key) - base;
       od[t] = none ? __int_as_float(0x7f800000) : (squared ? key_d2(key) : sqrtf(key_d2(key)));
     }
     __syncwarp();
@@ -418,7 +418,7 @@ struct SelectTopK : TopKBase {
     theta = sqrtf(key_d2(thr));
   }
 
-  __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int lane) {
+  __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int32_t base, int lane) {
     flush(lane);
     __syncwarp();
     for (int i = nbuf + lane; i < LL; i += 32) buf[i] = kKeyMax;
@@ -427,7 +427,7 @@ struct SelectTopK : TopKBase {
     for (int t = lane; t < k; t += 32) {
       const uint64_t key = buf[t];
       const bool none = key == kKeyMax;
-      oi[t] = none ? -1 : key_idx(key);
+      oi[t] = none ? -1 : key_idx(key) - base;
       od[t] = none ? __int_as_float(0x7f800000) : (squared ? key_d2(key) : sqrtf(key_d2(key)));
     }
     __syncwarp();
@@ -634,7 +634,7 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, L, WARPS>())
     };
 
     const int nr = a.rlen[qc];
-    const int32_t *rl = a.rlist + (int64_t)qc * a.Rs;
+    const int32_t *rl = a.rlist + (a.rl_base ? a.rl_base[qc] : (int64_t)qc * a.Rs);
     for (int base = 0; base < nr; base += 32) {
       const int j = base + lane;
       int rs = 0;
@@ -730,7 +730,8 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, L, WARPS>())
       }
     }
     tk.flush(lane);
-    tk.write_out(a.out_idx + q * a.k, a.out_dist + q * a.k, a.squared, lane);
+    tk.write_out(a.out_idx + q * a.k, a.out_dist + q * a.k, a.squared,
+                 a.qc_ref_base ? (int32_t)a.qc_ref_base[qc] : 0, lane);
     if (a.counters) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {

@@ -116,3 +116,39 @@ def test_pack_indexdist_layout():
     raw = rec.view(np.int32).reshape(-1)
     assert raw[0] == 3 and raw[2] == 1 and raw[4] == 0 and raw[6] == -1
     assert rec["dist"][0, 1] == 2.0 and np.isinf(rec["dist"][1, 1])
+
+
+def _call_batched(qo, ro, ncloud, d, k, opt=None):
+    lib = _lib.load()
+    qo = np.ascontiguousarray(qo, np.int64)
+    ro = np.ascontiguousarray(ro, np.int64)
+    return lib.knn_join_batched_device(None, qo.ctypes.data_as(ctypes.c_void_p), None,
+                                       ro.ctypes.data_as(ctypes.c_void_p), ncloud, d, k, None,
+                                       None, None if opt is None else ctypes.byref(opt), None,
+                                       None)
+
+
+@pytest.mark.parametrize("qo,ro,ncloud,d,k", [
+    ([0, 10, 5], [0, 10, 5], 2, 3, 4),      # decreasing offsets
+    ([1, 10], [0, 10], 1, 3, 4),            # offsets not starting at 0
+    ([0, 10], [0, 10], 1, 0, 4),            # d = 0
+    ([0, 10], [0, 10], 1, 33, 4),           # d above the batched limit
+    ([0, 10], [0, 10], 1, 3, 257),          # k above the batched limit
+    ([0, 10], [0, 10], -1, 3, 4),           # negative cloud count
+    ([0, 10], [0, 10], 1, 3, 4),            # null device pointers
+])
+def test_batched_bad_arguments_rejected(qo, ro, ncloud, d, k):
+    assert _call_batched(qo, ro, ncloud, d, k) == _lib.KNN_EINVAL
+    assert _lib.load().knn_last_error()
+
+
+def test_batched_empty_batches_ok_without_gpu():
+    assert _call_batched([0], [0], 0, 3, 4) == _lib.KNN_OK
+    assert _call_batched([0, 0, 0], [0, 5, 9], 2, 3, 4) == _lib.KNN_OK
+
+
+def test_batched_bad_options_rejected():
+    for field, val in [("flags", 4), ("rep_trials", 0)]:
+        o = _lib.default_options()
+        setattr(o, field, val)
+        assert _call_batched([0, 10], [0, 10], 1, 3, 4, opt=o) == _lib.KNN_EINVAL, field
