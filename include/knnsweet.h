@@ -45,8 +45,11 @@ extern "C" {
 
 /* Precision forms. */
 #define KNN_FP32 0        /* plain FP32 pruned join                          */
-#define KNN_BF16_REFINE 1 /* BF16 tensor-core distances, FP32 re-rank of the
-                             top k+margin, FP64 re-check of k-th ties         */
+#define KNN_BF16_REFINE 1 /* BF16 tensor-core distance tiles with error
+                             bounds, exact FP32 re-rank of the pairs the
+                             bounds keep, FP64 re-check of the k-th boundary
+                             (1 <= d <= 256; the neighbour set is the one an
+                             FP64 join gives)                                */
 
 /* Option flags. */
 #define KNN_SQUARED_DIST 1 /* out_dist holds squared distances |q - r|^2     */
@@ -72,7 +75,8 @@ typedef struct knn_options {
   uint32_t seed;      /* glibc srand() seed used to draw representative rows */
   int32_t rep_trials; /* random draws compared by pairwise spread            */
   int32_t precision;  /* KNN_FP32 or KNN_BF16_REFINE                          */
-  int32_t margin;     /* extra candidates re-ranked by the BF16 form         */
+  int32_t margin;     /* BF16 form: re-ranking reserve; each query keeps up to
+                         2 (k + margin) + 128 bound pairs before compacting */
   int32_t autotune;   /* batched form: pick tiles per cloud-size bucket      */
   int32_t flags;      /* KNN_SQUARED_DIST | KNN_NO_TENSOR_CORES, or 0        */
   int32_t lloyd_iters;/* representative refinement: after the draw, this many
@@ -102,7 +106,9 @@ typedef struct knn_stats {
   int32_t sreps_used;
   int32_t kernels_launched; /* device kernels this call enqueued (a radix sort
                                counts as one)                                 */
-  int32_t reserved;
+  int32_t refine_fallbacks; /* BF16 form: queries whose kept candidates did
+                               not fit the re-ranking buffer and went to the
+                               FP32 scan instead                              */
 } knn_stats;
 
 /* Fill `opt` with the defaults listed above. */

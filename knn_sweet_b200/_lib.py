@@ -59,7 +59,7 @@ class KnnStats(ctypes.Structure):
         ("qreps_used", ctypes.c_int32),
         ("sreps_used", ctypes.c_int32),
         ("kernels_launched", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("refine_fallbacks", ctypes.c_int32),
     ]
 
     def as_dict(self) -> dict:

@@ -32,8 +32,10 @@ NVCC_FLAGS = ARCH + [
     "-Xcompiler", "-Wall", "-I", str(ROOT / "include"),
 ]
 
-CU_SOURCES = ["api.cu", "build_index.cu", "scan.cu", "backward.cu", "noalloc.cu", "assign_tc.cu", "batched.cu"]
-HEADERS = ["common.cuh", "kernels.cuh", "glibc_rand.h", "tc_common.cuh", "bounds.cuh"]
+CU_SOURCES = ["api.cu", "build_index.cu", "scan.cu", "backward.cu", "noalloc.cu", "assign_tc.cu", "batched.cu",
+              "tile_search.cu"]
+HEADERS = ["common.cuh", "kernels.cuh", "glibc_rand.h", "tc_common.cuh", "bounds.cuh",
+           "warp_select.cuh"]
 
 
 def nvcc() -> str:

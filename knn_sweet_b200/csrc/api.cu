@@ -327,6 +327,10 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
   const bool self = (q == r) && (m == n);
   int Rs = o.sreps > 0 ? o.sreps : default_reps(n);
   int Rq = o.qreps > 0 ? o.qreps : (self ? Rs : default_reps(m));
+  // the tensor-core tiles hold 128 queries of one query cluster: by default
+  // the BF16 form sizes the query clusters to fill them
+  if (o.qreps <= 0 && !self && o.precision == KNN_BF16_REFINE && tile_search_supported(d, k, o.margin))
+    Rq = (int)std::min<int64_t>(KNN_MAX_REPS, std::max<int64_t>(1, (m + 127) / 128));
   if (Rs > n) Rs = (int)n;
   if (Rq > m) Rq = (int)m;
   const bool share = self && Rq == Rs;
@@ -348,10 +352,11 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
     *outp = p;
     return KNN_OK;
   };
-  // [0] work counter, [1..5] statistics, [6] device error flag
+  // [0] work counter, [1..5] statistics, [6] device error flag, [7] tile
+  // counter, [8..11] tile statistics, [12] count of slots left to the scan
   unsigned long long *ctr;
-  KNN_TRY(ar.alloc(&ctr, 7));
-  KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, 7 * sizeof(unsigned long long), s));
+  KNN_TRY(ar.alloc(&ctr, 13));
+  KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, 13 * sizeof(unsigned long long), s));
   int *dev_err = reinterpret_cast<int *>(ctr + 6);
   const bool use_tc = (o.flags & KNN_NO_TENSOR_CORES) == 0;
 
@@ -396,6 +401,64 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
                                k, d, theta0, rlist, rlen, s));
   KNN_TRY(evs.record(1, s));
 
+  // BF16+refine form: tensor-core tiles over the same candidate lists; the
+  // FP32 scan below then runs only for the queries the tiles hand back.
+  int grid = 0, cap = 0, P = 0;
+  size_t smem = 0;
+  const bool tiles = o.precision == KNN_BF16_REFINE && tile_search_supported(d, k, o.margin) &&
+                     tile_search_geometry(d, k, o.margin, num_sms, &grid, &cap, &P, &smem) ==
+                         KNN_OK;
+  int32_t *fb_slots = nullptr;
+  unsigned *fb_count = reinterpret_cast<unsigned *>(ctr + 12);
+  if (tiles) {
+    grid = (int)std::min<int64_t>(grid, m / 128 + Rq + 1);
+    int32_t *tile_list, *ntiles;
+    float2 *buf_lu;
+    int32_t *buf_pos;
+    const size_t slots = (size_t)grid * 128 * cap;
+    KNN_TRY(ar.alloc(&tile_list, (size_t)4 * (m / 128 + Rq + 1)));
+    KNN_TRY(ar.alloc(&ntiles, 1));
+    KNN_TRY(ar.alloc(&buf_lu, slots));
+    KNN_TRY(ar.alloc(&buf_pos, slots));
+    KNN_TRY(ar.alloc(&fb_slots, (size_t)m));
+    KNN_TRY(launch_tile_list(qset.off, Rq, tile_list, ntiles, s));
+    TileArgs t{};
+    t.qrows = Qp;
+    t.dp4 = dp4s;
+    t.d = d;
+    t.KD = 16;
+    while (t.KD < d) t.KD <<= 1;
+    t.qorder = qset.perm;
+    t.tiles = tile_list;
+    t.ntiles = ntiles;
+    t.srows = srows;
+    t.sidx = sidx;
+    t.rrows = Rp;
+    t.soff = sset.off;
+    t.sdist = sdist;
+    t.cmin = cmin;
+    t.cmax = cmax;
+    t.sreps = sset.reps;
+    t.rlist = rlist;
+    t.rlen = rlen;
+    t.Rs = Rs;
+    t.theta0 = theta0;
+    t.k = k;
+    t.cap = cap;
+    t.P = P;
+    t.squared = (o.flags & KNN_SQUARED_DIST) != 0;
+    t.buf_lu = buf_lu;
+    t.buf_pos = buf_pos;
+    t.out_idx = out_idx;
+    t.out_dist = out_dist;
+    t.work = ctr + 7;
+    t.fb_slots = fb_slots;
+    t.fb_count = fb_count;
+    t.err = dev_err;
+    t.counters = ctr + 8;
+    KNN_TRY(launch_tile_search(t, grid, smem, s));
+  }
+
   ScanArgs a{};
   a.qrows = Qp;
   a.qorder = qset.perm;
@@ -422,18 +485,24 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
   a.out_dist = out_dist;
   a.work_counter = ctr;
   a.counters = ctr + 1;
+  if (tiles) {
+    a.slot_list = fb_slots;
+    a.slot_count = fb_count;
+  }
   KNN_TRY(launch_scan(a, num_sms, s));
   KNN_TRY(evs.record(2, s));
 
   if (st) {
-    unsigned long long h[7];
+    unsigned long long h[13];
     KNN_CUDA_TRY(cudaMemcpyAsync(h, ctr, sizeof h, cudaMemcpyDeviceToHost, s));
     KNN_CUDA_TRY(cudaStreamSynchronize(s));
     if (static_cast<int>(h[6] & 0xffffffffu) != 0) {
       set_error("a bounded device wait gave up (tensor-core pipeline)");
       return KNN_ETIMEOUT;
     }
-    st->dist_evals = (int64_t)h[1];
+    st->dist_evals = (int64_t)(h[1] + h[8] + h[9]);
+    st->refine_rechecks = (int64_t)h[10];
+    st->refine_fallbacks = (int32_t)h[11];
     st->clusters_visited = (int64_t)h[2];
     st->clusters_pruned = (int64_t)h[3];
     st->topk_candidates = (int64_t)h[4];

@@ -28,6 +28,8 @@ struct ScanArgs {
                             // in rlist (null: qc * Rs)
   const int64_t *qc_ref_base;  // batched form: subtracted from every output
                                // index of query cluster qc (null: 0)
+  const int32_t *slot_list;    // optional: scan only these slots ...
+  const unsigned *slot_count;  // ... *slot_count of them (device count)
   int Rs;
   int32_t *out_idx;         // m x k
   float *out_dist;          // m x k
@@ -72,5 +74,44 @@ int launch_bounds_filter(const float *drr, int Rq, int Rs, const float *qrad,
                          float *theta0, int32_t *rlist, int32_t *rlen,
                          cudaStream_t s);
 int launch_scan(const ScanArgs &a, int num_sms, cudaStream_t s);
+
+// Arguments of the BF16 tensor-core tile search with FP32 re-ranking
+// (tile_search.cu).
+struct TileArgs {
+  const float4 *qrows;       // m x dp4 queries, original order
+  int dp4, d, KD;            // row stride (float4), width, padded MMA K
+  const int32_t *qorder;     // slot -> query row (grouped by query cluster)
+  const int32_t *tiles;      // per tile: {query cluster, first slot, count,
+                             // slot of the centre point}
+  const int32_t *ntiles;     // device: number of tiles
+  const float4 *srows;       // n x dp4 reference rows, cluster-contiguous
+  const int32_t *sidx;       // n: original reference row
+  const float4 *rrows;       // n x dp4 reference rows, original order
+  const int32_t *soff;       // Rs + 1
+  const float *sdist;        // n: d(s, Rs), ascending within each cluster
+  const float *cmin, *cmax;  // Rs: smallest / largest member distance
+  const float4 *sreps;       // Rs x dp4 reference representatives
+  const int32_t *rlist;      // Rq x Rs surviving clusters, nearest first
+  const int32_t *rlen;       // Rq
+  int Rs;
+  const float *theta0;       // Rq: k-th distance bound per query cluster
+  int k, cap, P;             // k; buffer entries per query; sort scratch (pow2)
+  bool squared;
+  float2 *buf_lu;            // grid x 128 x cap: (lower, upper) bound pairs
+  int32_t *buf_pos;          // grid x 128 x cap: cluster-layout positions
+  int32_t *out_idx;
+  float *out_dist;
+  unsigned long long *work;  // tile counter, zeroed
+  int32_t *fb_slots;         // slots left to the FP32 scan
+  unsigned *fb_count;
+  int *err;                  // set when a bounded wait gives up
+  unsigned long long *counters;  // [tensor pairs, refined, fp64 rechecks, fallbacks]
+};
+bool tile_search_supported(int d, int k, int margin);
+int tile_search_geometry(int d, int k, int margin, int num_sms, int *grid, int *cap, int *P,
+                         size_t *smem);
+int launch_tile_list(const int32_t *qoff, int Rq, int32_t *tiles, int32_t *ntiles,
+                     cudaStream_t s);
+int launch_tile_search(const TileArgs &a, int grid, size_t smem, cudaStream_t s);
 
 }  // namespace knnsweet

@@ -33,21 +33,9 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "warp_select.cuh"
 
 namespace knnsweet {
-
-__device__ __forceinline__ uint64_t shfl_xor64(uint64_t v, int m) {
-  uint32_t lo = __shfl_xor_sync(kFull, (uint32_t)v, m);
-  uint32_t hi = __shfl_xor_sync(kFull, (uint32_t)(v >> 32), m);
-  return ((uint64_t)hi << 32) | lo;
-}
-__device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) {
-  uint32_t lo = __shfl_sync(kFull, (uint32_t)v, src);
-  uint32_t hi = __shfl_sync(kFull, (uint32_t)(v >> 32), src);
-  return ((uint64_t)hi << 32) | lo;
-}
-__device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
-__device__ __forceinline__ uint64_t umax64(uint64_t a, uint64_t b) { return a < b ? b : a; }
 
 // ---------------------------------------------------------------------------
 // Register bitonic networks over 32*E keys, blocked layout: lane l holds
@@ -296,82 +284,6 @@ struct SmemTopK : TopKBase {
   }
 };
 
-// k-th smallest (1-based rank k, 1 <= k <= n) of the distinct keys s[0..n),
-// by one warp: radix selection with 8-bit digits, starting at the highest bit
-// in which the keys differ; `hist` is a 256-word shared-memory histogram.
-// (Inlined: an out-of-line call spilled the caller's registers around it.)
-__device__ __forceinline__ uint64_t warp_select_kth(const uint64_t *s, int n, int k,
-                                                 uint32_t *hist, int lane) {
-  uint64_t mn = kKeyMax, mx = 0;
-  for (int i = lane; i < n; i += 32) {
-    const uint64_t v = s[i];
-    mn = umin64(mn, v);
-    mx = umax64(mx, v);
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    mn = umin64(mn, shfl_xor64(mn, o));
-    mx = umax64(mx, shfl_xor64(mx, o));
-  }
-  if (mn == mx) return mn;
-  const int hb = 63 - __clzll((long long)(mn ^ mx));  // highest differing bit
-  uint64_t known = hb == 63 ? 0ull : (~0ull << (hb + 1));
-  uint64_t prefix = mn & known;
-  uint32_t need = (uint32_t)k;
-  int top = hb + 1;  // bits [0, top) still unknown
-  for (;;) {
-    const int shift = top > 8 ? top - 8 : 0;
-    const uint32_t dmask = (1u << (top - shift)) - 1u;
-    __syncwarp();
-#pragma unroll
-    for (int b = 0; b < 8; b++) hist[b * 32 + lane] = 0;
-    __syncwarp();
-    for (int i = lane; i < n; i += 32) {
-      const uint64_t v = s[i];
-      if ((v & known) == prefix) atomicAdd(&hist[(uint32_t)(v >> shift) & dmask], 1u);
-    }
-    __syncwarp();
-    // bin holding the need-th key: scan the bins 32 at a time
-    uint32_t base = 0, before = 0, cnt_b = 0;
-    int bin = -1;
-#pragma unroll 1
-    for (int j = 0; j < 8 && bin < 0; j++) {
-      const uint32_t h = hist[j * 32 + lane];
-      uint32_t incl = h;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += t;
-      }
-      const uint32_t total = __shfl_sync(kFull, incl, 31);
-      if (base + total >= need) {
-        const int wl = __ffs(__ballot_sync(kFull, base + incl >= need)) - 1;
-        bin = j * 32 + wl;
-        before = base + __shfl_sync(kFull, incl - h, wl);
-        cnt_b = __shfl_sync(kFull, h, wl);
-      }
-      base += total;
-    }
-    need -= before;
-    prefix |= (uint64_t)bin << shift;
-    known |= (uint64_t)dmask << shift;
-    if (shift == 0) return prefix;
-    if (cnt_b == 1) {  // the only key with this prefix
-      uint64_t found = 0;
-      bool f = false;
-      for (int i = lane; i < n; i += 32) {
-        const uint64_t v = s[i];
-        if ((v & known) == prefix) {
-          found = v;
-          f = true;
-        }
-      }
-      return shfl64(found, __ffs(__ballot_sync(kFull, f)) - 1);
-    }
-    top = shift;
-  }
-}
-
 // Top-k as an unsorted candidate set in shared memory (capacity 2L).  When it
 // fills, the exact k-th key is found by warp_select_kth, the set is compacted
 // to the k best and the threshold drops to that key; the k results are sorted
@@ -583,7 +495,12 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, L, WARPS>())
     long long slot = 0;
     if (lane == 0) slot = (long long)atomicAdd(a.work_counter, 1ull);
     slot = __shfl_sync(kFull, slot, 0);
-    if (slot >= a.m) break;
+    if (a.slot_list) {
+      if (slot >= (long long)*a.slot_count) break;
+      slot = a.slot_list[slot];
+    } else if (slot >= a.m) {
+      break;
+    }
     const int64_t q = a.qorder[slot];
     const int qc = a.slot_cl[slot];
     QueryRow<DP4, IDXROW> qr;

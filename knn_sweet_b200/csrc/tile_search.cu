@@ -1,0 +1,772 @@
+// tile_search.cu -- the BF16+refine form of the join's search: tensor-core
+// (tcgen05) distance tiles with rigorous error bounds, exact FP32 re-ranking
+// and an FP64 re-check of the k-th boundary.
+//
+// It replaces the per-query scan (KNNQuery_base, src/knnjoin.cu:762-858) for
+// the same clusters, bounds and candidate cluster lists: the reference
+// computes every surviving distance in FP32 on CUDA cores; here a CTA takes
+// a tile of up to 128 queries of one query cluster and streams the members
+// of that cluster's candidate list (nearest cluster first) through a
+// 128 x 128 x KD BF16 MMA with FP32 accumulation in TMEM:
+//   - rows are centred on one query point of the cluster before rounding to
+//     BF16, so the rounded values (and their errors) are small; data on an
+//     integer grid stays exact;
+//   - for every (query, member) pair the epilogue turns the dot product into
+//     a lower bound L and an upper bound U of the exact squared distance,
+//         L, U = |a|^2 + |b|^2 -/+ slack - 2 acc -/+ delta,
+//     where delta bounds the BF16 rounding (|a| |b - b~| + |a - a~| |b~|)
+//     and the tensor-core accumulation, from per-row norms computed in FP32;
+//   - each query keeps, in a global-memory buffer, every pair whose L is at
+//     most the k-th smallest U seen so far (initially theta0^2, the cluster's
+//     k-th distance bound): no pair outside can be among the k nearest.
+//     When a buffer fills, a warp selects the k-th U (radix select) and
+//     compacts it;
+//   - at the end a warp per query recomputes the kept pairs exactly in FP32
+//     (the same arithmetic as the FP32 scan), selects the k smallest keys
+//     (d^2, index), and re-decides every key within the FP32 rounding band of
+//     the k-th in FP64 (ties to the lower index).  The neighbour set is
+//     therefore the one an FP64 join gives.
+// A query whose buffer cannot hold its kept pairs (for example thousands of
+// duplicate points at the boundary) is handed to the FP32 scan.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "tc_common.cuh"
+#include "warp_select.cuh"
+
+namespace knnsweet {
+
+namespace {
+
+// Optional phase timers (build with -DKNN_TILE_PROFILE=1): thread 0 of every
+// CTA adds the clock cycles between its barriers to tile_prof[phase].
+#ifndef KNN_TILE_PROFILE
+#define KNN_TILE_PROFILE 0
+#endif
+#if KNN_TILE_PROFILE
+__device__ unsigned long long tile_prof[16];
+#define TILE_PROF(i)                                  \
+  do {                                                \
+    if (tid == 0) {                                   \
+      const long long now_ = clock64();               \
+      prof[i] += (unsigned long long)(now_ - prof_t); \
+      prof_t = now_;                                  \
+    }                                                 \
+  } while (0)
+#else
+#define TILE_PROF(i) \
+  do {               \
+  } while (0)
+#endif
+
+constexpr int kTM = 128;  // queries per tile: TMEM lanes, threads per CTA
+constexpr int kTN = 128;  // member rows per chunk: TMEM columns
+
+// Tile list: every query cluster's slots in tiles of up to kTM, as
+// {query cluster, first slot, count, slot of the cluster's centre point}.
+// The centre is the cluster's first slot: the query nearest its
+// representative.  One block of 1024 threads, each owning a run of clusters.
+__global__ void __launch_bounds__(1024)
+    tile_list_kernel(const int32_t *__restrict__ qoff, int Rq, int32_t *__restrict__ tiles,
+                     int32_t *__restrict__ ntiles) {
+  __shared__ int wsum[32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int per = (Rq + 1023) / 1024;
+  const int c0 = min(Rq, tid * per), c1 = min(Rq, c0 + per);
+  int local = 0;
+  for (int c = c0; c < c1; c++) local += (qoff[c + 1] - qoff[c] + kTM - 1) / kTM;
+  int incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const int v = wsum[lane];
+    int iv = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(kFull, iv, o);
+      if (lane >= o) iv += t;
+    }
+    wsum[lane] = iv - v;
+  }
+  __syncthreads();
+  int pos = wsum[warp] + incl - local;
+  for (int c = c0; c < c1; c++) {
+    const int size = qoff[c + 1] - qoff[c];
+    for (int s = 0; s < size; s += kTM) {
+      tiles[4 * pos + 0] = c;
+      tiles[4 * pos + 1] = qoff[c] + s;
+      tiles[4 * pos + 2] = min(kTM, size - s);
+      tiles[4 * pos + 3] = qoff[c];
+      pos++;
+    }
+  }
+  if (tid == 1023) *ntiles = pos;
+}
+
+// Rows r of a 128-row tile, centred on sc, rounded to BF16 into the
+// core-matrix layout of tc_common.cuh; per row the sums
+//   o_n = sum v^2, o_e = sum (v - bf16(v))^2, o_t = sum bf16(v)^2
+// of the centred FP32 values v.  rowptr(r) gives the row (nullptr: zeros).
+// G = KD/8 consecutive threads share a row (one 16-byte group each).
+template <class RowPtr>
+__device__ __forceinline__ void stage_tile(unsigned char *tile, const float *sc, int KD, int d,
+                                           int dp4, RowPtr rowptr, float *o_n, float *o_e,
+                                           float *o_t) {
+  const int G = KD >> 3;
+  for (int t = threadIdx.x; t < kTM * G; t += kTM) {
+    const int r = t / G, g = t - r * G, k0 = g << 3;
+    const float4 *row = rowptr(r);
+    float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f), c1 = c0;
+    if (row) {
+      if ((k0 >> 2) < dp4) c0 = row[k0 >> 2];
+      if ((k0 >> 2) + 1 < dp4) c1 = row[(k0 >> 2) + 1];
+    }
+    const float v[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+    float sn = 0.0f, se = 0.0f, st = 0.0f;
+    __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      const int kk = k0 + e;
+      const float x = (row && kk < d) ? __fsub_rn(v[e], sc[kk]) : 0.0f;
+      h[e] = __float2bfloat16_rn(x);
+      const float xr = __bfloat162float(h[e]);
+      const float df = __fsub_rn(x, xr);
+      sn = __fmaf_rn(x, x, sn);
+      se = __fmaf_rn(df, df, se);
+      st = __fmaf_rn(xr, xr, st);
+    }
+    *reinterpret_cast<uint4 *>(tile + tc::tile_offset(r, k0, KD)) =
+        *reinterpret_cast<const uint4 *>(h);
+    for (int o = G >> 1; o > 0; o >>= 1) {
+      sn += __shfl_xor_sync(kFull, sn, o);
+      se += __shfl_xor_sync(kFull, se, o);
+      st += __shfl_xor_sync(kFull, st, o);
+    }
+    if (g == 0) {
+      o_n[r] = sn;
+      o_e[r] = se;
+      o_t[r] = st;
+    }
+  }
+}
+
+// Keeps the entries of a bound buffer (lu, pos: n entries in shared memory)
+// whose lower bound is at most the k-th smallest upper bound -- no entry
+// beyond it can be among the k nearest; in place, by one warp.  Returns the
+// count kept and that bound.  Needs n >= k.
+__device__ __forceinline__ int compact_bounds(float2 *lu, int32_t *pos, int n, int k,
+                                              uint32_t *hist, int lane, float *uk_out) {
+  const float uk = __uint_as_float(
+      warp_select_kth_u32(reinterpret_cast<const uint32_t *>(lu) + 1, 2, n, k, hist, lane));
+  int w = 0;
+  for (int b0 = 0; b0 < n; b0 += 32) {
+    const int i = b0 + lane;
+    float2 v = make_float2(0.0f, 0.0f);
+    int32_t p = 0;
+    if (i < n) {
+      v = lu[i];
+      p = pos[i];
+    }
+    const bool keep = i < n && v.x <= uk;
+    const unsigned bm = __ballot_sync(kFull, keep);
+    if (keep) {
+      const int o = w + __popc(bm & ((1u << lane) - 1u));
+      lu[o] = v;
+      pos[o] = p;
+    }
+    w += __popc(bm);
+  }
+  __syncwarp();
+  *uk_out = uk;
+  return w;
+}
+
+// Copies n buffer entries between global and shared memory, by one warp.
+__device__ __forceinline__ void copy_entries(float2 *dlu, int32_t *dpos, const float2 *slu,
+                                             const int32_t *spos, int n, int lane) {
+  __syncwarp();
+  for (int i = lane; i < n; i += 32) {
+    dlu[i] = slu[i];
+    dpos[i] = spos[i];
+  }
+  __syncwarp();
+}
+
+// Exact squared distance in FP32 over the first d columns, in column order:
+// the value the FP32 scan computes for the same pair.
+__device__ __forceinline__ float dist2_cols(const float *__restrict__ q,
+                                            const float *__restrict__ r, int d) {
+  float acc = 0.0f;
+  for (int c = 0; c < d; c++) {
+    const float t = __fsub_rn(q[c], r[c]);
+    acc = __fmaf_rn(t, t, acc);
+  }
+  return acc;
+}
+
+__device__ __forceinline__ double dist2_cols_f64(const float *__restrict__ q,
+                                                 const float *__restrict__ r, int d) {
+  double acc = 0.0;
+  for (int c = 0; c < d; c++) {
+    const double t = (double)q[c] - (double)r[c];
+    acc = fma(t, t, acc);
+  }
+  return acc;
+}
+
+// FP32 rounding band of a squared distance D computed by dist2_cols.
+__device__ __forceinline__ float band_eps(float D, int d) {
+  return (float)(d + 4) * 5.9604645e-8f * D;
+}
+
+__global__ void __launch_bounds__(kTM)
+    tile_search_kernel(const TileArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int KD = a.KD, d = a.d, dp4 = a.dp4, k = a.k, cap = a.cap, P = a.P;
+  (void)P;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  unsigned char *sa = smem;                                      // kTM x KD bf16
+  unsigned char *sb = sa + tc::tile_bytes(kTM, KD);              // kTN x KD bf16
+  float *sc = reinterpret_cast<float *>(sb + tc::tile_bytes(kTN, KD));  // KD
+  float4 *s_col = reinterpret_cast<float4 *>(sc + KD);          // kTN column scalars
+  float *s_n = reinterpret_cast<float *>(s_col + kTN);           // kTN row sums
+  float *s_e = s_n + kTN;
+  float *s_t = s_e + kTN;
+  int32_t *s_pos = reinterpret_cast<int32_t *>(s_t + kTN);      // kTN member positions
+  int32_t *s_rlo = s_pos + kTN;                                  // kTN run starts
+  int32_t *s_roff = s_rlo + kTN;                                 // kTN run offsets
+  float *s_cmin = reinterpret_cast<float *>(s_roff + kTN);       // kTN per batch cluster
+  float *s_cmax = s_cmin + kTN;
+  float *s_ck = s_cmax + kTN;                                    // k-th member distance
+  uint32_t *s_blo = reinterpret_cast<uint32_t *>(s_ck + kTN);    // run bounds (float bits)
+  uint32_t *s_bhi = s_blo + kTN;
+  int32_t *s_wsum = reinterpret_cast<int32_t *>(s_bhi + kTN);    // 4 warp sums
+  uint32_t *s_wmax = reinterpret_cast<uint32_t *>(s_wsum + 4);   // [1]: run total
+  uint32_t *hist = s_wmax + 4;                                   // 4 x 256
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(hist + 4 * 256);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 1);
+  int32_t *s_tile = reinterpret_cast<int32_t *>(tmem_slot + 1);  // 4 ints
+  // per warp: one query's buffer (cap bound pairs, cap positions)
+  const size_t wofs = ((size_t)(reinterpret_cast<unsigned char *>(s_tile + 4) - smem) + 15) &
+                      ~(size_t)15;
+  unsigned char *wbase = smem + wofs + (size_t)warp * cap * 12;
+  float2 *w_lu = reinterpret_cast<float2 *>(wbase);
+  int32_t *w_pos = reinterpret_cast<int32_t *>(wbase + (size_t)cap * 8);
+  uint32_t *whist = hist + warp * 256;
+
+  if (warp == 0) tc::tmem_alloc(tmem_slot, kTN);
+  if (tid == 0) tc::mbar_init(mbar, 1);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t idesc = tc::make_idesc_bf16(kTM, kTN);
+  const uint32_t a_base = tc::smem_u32(sa), b_base = tc::smem_u32(sb);
+  const uint32_t sbo = (uint32_t)KD * 16;
+  // relative slack of the FP32 norms, centring and bound arithmetic
+  const float kap = (float)(d + 32) * 5.9604645e-8f;
+  // tensor-core accumulation error per unit of |a~| |b~|
+  const float gtc = (float)(KD + 4) * 2.3841858e-7f;
+  // relative slack of the triangle-inequality tests (FP32 rounding of the
+  // representative and member distances)
+  const float tol = bound_tol(d);
+  const size_t row0 = (size_t)blockIdx.x * kTM;
+  float2 *my_lu = a.buf_lu + (row0 + tid) * cap;
+  int32_t *my_pos = a.buf_pos + (row0 + tid) * cap;
+  uint32_t phase = 0;
+  bool ok = true;
+  unsigned long long pairs = 0, refined = 0, rechecks = 0, fallbacks = 0;
+#if KNN_TILE_PROFILE
+  unsigned long long prof[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  long long prof_t = clock64();
+#endif
+
+  for (;;) {
+    if (tid == 0) {
+      const unsigned long long w = atomicAdd(a.work, 1ull);
+      if (w < (unsigned long long)*a.ntiles) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) s_tile[i] = a.tiles[4 * w + i];
+      } else {
+        s_tile[0] = -1;
+      }
+    }
+    __syncthreads();
+    const int qc = s_tile[0];
+    if (qc < 0) break;
+    const int s0 = s_tile[1], cnt = s_tile[2];
+    const float *cen = reinterpret_cast<const float *>(a.qrows +
+                                                       (size_t)a.qorder[s_tile[3]] * dp4);
+    for (int kk = tid; kk < KD; kk += kTM) sc[kk] = kk < d ? cen[kk] : 0.0f;
+    __syncthreads();
+    stage_tile(
+        sa, sc, KD, d, dp4,
+        [&](int r) -> const float4 * {
+          return r < cnt ? a.qrows + (size_t)a.qorder[s0 + r] * dp4 : nullptr;
+        },
+        s_n, s_e, s_t);
+    __syncthreads();
+    const bool valid = tid < cnt;
+    const float na = s_n[tid];
+    const float qa = 2.02f * sqrtf(na);
+    const float qb = 2.02f * (sqrtf(s_e[tid]) + gtc * sqrtf(s_t[tid]));
+    const float th = a.theta0[qc];
+    float tau = th * th * 1.0009765625f;
+    int n = 0;
+    bool ovf = false;
+    __syncthreads();  // the row sums are reused for the member rows below
+    TILE_PROF(0);
+
+    const int32_t *rl = a.rlist + (size_t)qc * a.Rs;
+    const int nl = a.rlen[qc];
+    int lim = min(cap - kTN, k + 32);  // compact when the buffer passes this
+    float th_q = sqrtf(tau);           // this query's k-th distance bound
+    // Candidate clusters in batches of 128, nearest first.  One MMA of the
+    // tile's queries against the batch's representatives (same centring and
+    // bounds as the member pairs) gives every query an interval
+    // [dl, du] for d(q, Rc).  Then, per query:
+    //   - theta_q <= du + (k-th member distance of c) for any cluster with
+    //     at least k members (those k members are within that distance);
+    //   - cluster c is needed only if dl - cmax(c) <= theta_q, and then only
+    //     its members with d(s,Rc) in [dl - theta_q, du + theta_q]
+    //     (triangle inequality), one contiguous run of the sorted members.
+    // The tile streams, per cluster, the union of its queries' runs.
+    for (int jb = 0; jb < nl && ok; jb += kTN) {
+      const int nb = min(kTN, nl - jb);
+      stage_tile(
+          sb, sc, KD, d, dp4,
+          [&](int r) -> const float4 * {
+            return r < nb ? a.sreps + (size_t)rl[jb + r] * dp4 : nullptr;
+          },
+          s_n, s_e, s_t);
+      if (tid < nb) {
+        const int c = rl[jb + tid];
+        const int c0 = a.soff[c], sz = a.soff[c + 1] - c0;
+        s_cmin[tid] = a.cmin[c];
+        s_cmax[tid] = a.cmax[c];
+        s_ck[tid] = sz >= k ? a.sdist[c0 + k - 1] : __int_as_float(0x7f800000);
+        s_blo[tid] = 0x7f800000u;
+        s_bhi[tid] = 0u;
+      }
+      tc::fence_proxy_async_smem();
+      tc::fence_before_sync();
+      __syncthreads();
+      tc::fence_after_sync();
+      if (tid == 0) {
+        for (int st = 0; st < KD / 16; st++) {
+          const uint64_t ad = tc::make_desc(a_base + 256u * st, 128u, sbo);
+          const uint64_t bd = tc::make_desc(b_base + 256u * st, 128u, sbo);
+          tc::mma_bf16(tmem, ad, bd, idesc, st > 0);
+        }
+        tc::mma_commit(mbar);
+      }
+      s_col[tid] = tid < nb ? make_float4(s_n[tid], sqrtf(s_e[tid]), sqrtf(s_t[tid]), 0.0f)
+                            : make_float4(__int_as_float(0x7f800000), 0.0f, 0.0f, 0.0f);
+      ok = tc::mbar_wait(mbar, phase);
+      phase ^= 1u;
+      ok = __syncthreads_and(ok) != 0;
+      if (!ok) break;
+      tc::fence_after_sync();
+      const bool act = valid && !ovf;
+      // pass 1: tighter theta_q from clusters with >= k members
+      for (int cc = 0; cc < nb; cc += 32) {
+        float acc[32];
+        tc::tmem_ld_32x32(lane_base + (uint32_t)cc, acc);
+        if (act) {
+#pragma unroll
+          for (int jj = 0; jj < 32; jj++) {
+            const float4 cv = s_col[cc + jj];
+            const float base = na + cv.x;
+            const float t2 = -2.0f * acc[jj];
+            const float dl = __fmaf_rn(qa, cv.y, qb * cv.z);
+            const float U = __fmaf_rn(base, 1.0f + kap, t2) + dl;
+            const float ub = (sqrtf(fmaxf(U, 0.0f)) + s_ck[cc + jj]) * (1.0f + tol);
+            if (cc + jj < nb) th_q = fminf(th_q, ub);
+          }
+        }
+      }
+      if (act) tau = fminf(tau, th_q * th_q * (1.0f + 4.0f * tol));
+      // pass 2: the clusters each query needs and the union of their runs
+      for (int cc = 0; cc < nb; cc += 32) {
+        float acc[32];
+        tc::tmem_ld_32x32(lane_base + (uint32_t)cc, acc);
+        if (act) {
+#pragma unroll
+          for (int jj = 0; jj < 32; jj++) {
+            const int col = cc + jj;
+            const float4 cv = s_col[col];
+            const float base = na + cv.x;
+            const float t2 = -2.0f * acc[jj];
+            const float dl = __fmaf_rn(qa, cv.y, qb * cv.z);
+            const float L = __fmaf_rn(base, 1.0f - kap, t2) - dl;
+            const float U = __fmaf_rn(base, 1.0f + kap, t2) + dl;
+            const float Dl = sqrtf(fmaxf(L, 0.0f)), Du = sqrtf(fmaxf(U, 0.0f));
+            const float sl = tol * (Du + th_q + s_cmax[col]) + 1.17549435e-38f;
+            if (col < nb && Dl - s_cmax[col] - sl <= th_q && Du + th_q + sl >= s_cmin[col]) {
+              atomicMin(&s_blo[col], __float_as_uint(fmaxf(Dl - th_q - sl, 0.0f)));
+              atomicMax(&s_bhi[col], __float_as_uint(Du + th_q + sl));
+            }
+          }
+        }
+      }
+      tc::fence_before_sync();
+      __syncthreads();  // TMEM and the member tile are reused below
+      tc::fence_after_sync();
+      // runs: the members of cluster tid whose d(s,Rc) is in [blo, bhi]
+      {
+        int lo = 0, len = 0;
+        if (tid < nb && s_blo[tid] <= s_bhi[tid]) {
+          const int c = rl[jb + tid];
+          const float lo_v = __uint_as_float(s_blo[tid]), hi_v = __uint_as_float(s_bhi[tid]);
+          int l = a.soff[c], h = a.soff[c + 1];
+          while (l < h) {  // first member with d(s,Rc) >= lo_v
+            const int md = (l + h) >> 1;
+            if (a.sdist[md] < lo_v) l = md + 1;
+            else h = md;
+          }
+          lo = l;
+          h = a.soff[c + 1];
+          while (l < h) {  // first member with d(s,Rc) > hi_v
+            const int md = (l + h) >> 1;
+            if (a.sdist[md] <= hi_v) l = md + 1;
+            else h = md;
+          }
+          len = l - lo;
+        }
+        int incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int t = __shfl_up_sync(kFull, incl, o);
+          if (lane >= o) incl += t;
+        }
+        if (lane == 31) s_wsum[warp] = incl;
+        __syncthreads();
+        int before = 0;
+        for (int w = 0; w < warp; w++) before += s_wsum[w];
+        s_rlo[tid] = lo;
+        s_roff[tid] = before + incl - len;
+        if (tid == kTM - 1) s_wmax[1] = (uint32_t)(before + incl);
+      }
+      __syncthreads();
+      const int total = (int)s_wmax[1];
+#if KNN_TILE_PROFILE
+      if (tid == 0) {
+        atomicAdd(&tile_prof[8], 1ull);
+        atomicAdd(&tile_prof[10], (unsigned long long)total);
+        if (jb == 0) {
+          atomicAdd(&tile_prof[11], 1ull);
+          atomicAdd(&tile_prof[12], (unsigned long long)nl);
+        }
+      }
+#endif
+      // the runs, concatenated, in chunks of kTN rows
+      for (int o = 0; o < total; o += kTN) {
+        const int nr = min(kTN, total - o);
+        stage_tile(
+            sb, sc, KD, d, dp4,
+            [&](int r) -> const float4 * {
+              if (r >= nr) return nullptr;
+              const int g = o + r;
+              int l = 0, h = kTN - 1;  // last run starting at or before g
+              while (l < h) {
+                const int md = (l + h + 1) >> 1;
+                if (s_roff[md] <= g) l = md;
+                else h = md - 1;
+              }
+              const int p = s_rlo[l] + (g - s_roff[l]);
+              s_pos[r] = p;
+              return a.srows + (size_t)p * dp4;
+            },
+            s_n, s_e, s_t);
+        tc::fence_proxy_async_smem();
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        TILE_PROF(1);
+        if (tid == 0) {
+          for (int st = 0; st < KD / 16; st++) {
+            const uint64_t ad = tc::make_desc(a_base + 256u * st, 128u, sbo);
+            const uint64_t bd = tc::make_desc(b_base + 256u * st, 128u, sbo);
+            tc::mma_bf16(tmem, ad, bd, idesc, st > 0);
+          }
+          tc::mma_commit(mbar);
+        }
+        // column scalars: |b|^2 (+inf on padding), |b - b~|, |b~|, position
+        s_col[tid] = tid < nr ? make_float4(s_n[tid], sqrtf(s_e[tid]), sqrtf(s_t[tid]),
+                                            __int_as_float(s_pos[tid]))
+                              : make_float4(__int_as_float(0x7f800000), 0.0f, 0.0f, 0.0f);
+        ok = tc::mbar_wait(mbar, phase);
+        phase ^= 1u;
+        ok = __syncthreads_and(ok) != 0;
+        if (!ok) break;
+        tc::fence_after_sync();
+        TILE_PROF(2);
+        for (int cc = 0; cc < nr; cc += 32) {
+          float acc[32];
+          tc::tmem_ld_32x32(lane_base + (uint32_t)cc, acc);
+          if (valid && !ovf) {
+#pragma unroll
+            for (int jj = 0; jj < 32; jj++) {
+              const float4 cv = s_col[cc + jj];
+              const float base = na + cv.x;
+              const float t2 = -2.0f * acc[jj];
+              const float dl = __fmaf_rn(qa, cv.y, qb * cv.z);
+              const float L = __fmaf_rn(base, 1.0f - kap, t2) - dl;
+              if (L <= tau && n < cap) {
+                const float U = __fmaf_rn(base, 1.0f + kap, t2) + dl;
+                my_lu[n] = make_float2(fmaxf(L, 0.0f), fmaxf(U, 0.0f));
+                my_pos[n] = __float_as_int(cv.w);
+                n++;
+              }
+            }
+          }
+        }
+        if (valid) pairs += (unsigned long long)nr;
+        TILE_PROF(3);
+        // buffers past their limit are compacted (tightening tau)
+        unsigned need = __ballot_sync(kFull, valid && !ovf && n > lim);
+        while (need) {
+          const int rr = __ffs(need) - 1;
+          need &= need - 1u;
+          const int nn = __shfl_sync(kFull, n, rr);
+          const size_t ro = (row0 + warp * 32 + rr) * cap;
+          float uk;
+          copy_entries(w_lu, w_pos, a.buf_lu + ro, a.buf_pos + ro, nn, lane);
+          const int kept = compact_bounds(w_lu, w_pos, nn, k, whist, lane, &uk);
+          copy_entries(a.buf_lu + ro, a.buf_pos + ro, w_lu, w_pos, kept, lane);
+          if (lane == rr) {
+            n = kept;
+            tau = fminf(tau, uk);
+            lim = min(cap - kTN, 2 * kept + 32);
+            if (kept > cap - kTN) ovf = true;
+          }
+        }
+        TILE_PROF(4);
+        tc::fence_before_sync();
+        __syncthreads();  // the member tile, TMEM and column scalars are reused
+        tc::fence_after_sync();
+        TILE_PROF(5);
+      }
+    }
+    if (!ok) break;
+    TILE_PROF(5);
+
+#if KNN_TILE_PROFILE
+    if (valid) {
+      atomicAdd(&tile_prof[13], (unsigned long long)(sqrtf(tau) * 1000.0f));
+      atomicAdd(&tile_prof[15], 1ull);
+    }
+#endif
+    // finish this warp's queries: exact re-ranking and the FP64 boundary,
+    // on a shared-memory copy of each query's buffer
+    for (int i = 0; i < 32; i++) {
+      const int row = warp * 32 + i;
+      if (row >= cnt) break;
+      const int nn = __shfl_sync(kFull, n, i);
+      bool fb = __shfl_sync(kFull, (int)ovf, i) != 0;
+      const int slot = s0 + row;
+      const int64_t q = a.qorder[slot];
+      const size_t ro = (row0 + row) * cap;
+      int m1 = nn;
+      if (!fb) {
+        copy_entries(w_lu, w_pos, a.buf_lu + ro, a.buf_pos + ro, m1, lane);
+        if (m1 > k) {
+          float uk;
+          m1 = compact_bounds(w_lu, w_pos, m1, k, whist, lane, &uk);
+        }
+      }
+      // exact FP32 keys, written over the bound pairs
+      uint64_t *keys = reinterpret_cast<uint64_t *>(w_lu);
+      const float *qf = reinterpret_cast<const float *>(a.qrows + (size_t)q * dp4);
+      if (!fb) {
+        for (int e = lane; e < m1; e += 32) {
+          const int p = w_pos[e];
+          const float d2 =
+              dist2_cols(qf, reinterpret_cast<const float *>(a.srows + (size_t)p * dp4), d);
+          keys[e] = make_key(d2, a.sidx[p]);
+        }
+        if (lane == 0) refined += (unsigned long long)m1;
+        __syncwarp();
+      }
+      // the k smallest keys plus every key inside the FP32 band of the k-th
+      // (compacted in place: keys[0..m2))
+      int m2 = m1;
+      if (!fb && m1 > k) {
+        const uint64_t kth = warp_select_kth(keys, m1, k, whist, lane);
+        const float Dk = key_d2(kth);
+        const float lim2 = Dk + 2.0f * band_eps(Dk, d);
+        int w = 0;
+        for (int b0 = 0; b0 < m1; b0 += 32) {
+          const int e = b0 + lane;
+          const uint64_t key = e < m1 ? keys[e] : kKeyMax;
+          const bool keep = e < m1 && key_d2(key) <= lim2;
+          const unsigned bm = __ballot_sync(kFull, keep);
+          __syncwarp();
+          if (keep) keys[w + __popc(bm & ((1u << lane) - 1u))] = key;
+          w += __popc(bm);
+        }
+        __syncwarp();
+        m2 = w;
+      }
+      int np2 = 32;
+      while (np2 < m2) np2 <<= 1;
+      if (!fb && np2 > cap) fb = true;
+      if (!fb) {
+        for (int e = m2 + lane; e < np2; e += 32) keys[e] = kKeyMax;
+        __syncwarp();
+        smem_bitonic_sort_rt(keys, np2, lane);
+        if (m2 > k) {
+          // keys at or above Dk - band were ranked in FP32 only to within
+          // rounding: order them again by (FP64 d^2, index)
+          const float Dk = key_d2(keys[k - 1]);
+          const float lo_v = Dk - 2.0f * band_eps(Dk, d);
+          int lo = 0;
+          for (int b0 = 0; b0 < m2; b0 += 32) {
+            const int e = b0 + lane;
+            lo += __popc(__ballot_sync(kFull, e < m2 && key_d2(keys[e]) < lo_v));
+          }
+          const int bsz = m2 - lo;
+          if (2 * bsz > cap || np2 + bsz > cap) {
+            fb = true;
+          } else {
+            double *d64 = reinterpret_cast<double *>(w_pos);
+            uint64_t *perm = keys + np2;
+            for (int e = lane; e < bsz; e += 32) {
+              const int32_t id = key_idx(keys[lo + e]);
+              d64[e] = dist2_cols_f64(
+                  qf, reinterpret_cast<const float *>(a.rrows + (size_t)id * dp4), d);
+            }
+            __syncwarp();
+            for (int e = lane; e < bsz; e += 32) {
+              const double de = d64[e];
+              const int32_t ie = key_idx(keys[lo + e]);
+              int rank = 0;
+              for (int f = 0; f < bsz; f++) {
+                const double df = d64[f];
+                const int32_t iff = key_idx(keys[lo + f]);
+                rank += (df < de || (df == de && iff < ie)) ? 1 : 0;
+              }
+              perm[rank] = keys[lo + e];
+            }
+            __syncwarp();
+            for (int e = lane; e < bsz; e += 32) keys[lo + e] = perm[e];
+            __syncwarp();
+            if (lane == 0) rechecks += (unsigned long long)bsz;
+          }
+        }
+      }
+      if (fb) {
+        if (lane == 0) {
+          a.fb_slots[atomicAdd(a.fb_count, 1u)] = slot;
+          fallbacks++;
+        }
+      } else {
+        int32_t *oi = a.out_idx + (size_t)q * k;
+        float *od = a.out_dist + (size_t)q * k;
+        for (int t = lane; t < k; t += 32) {
+          const uint64_t key = t < m2 ? keys[t] : kKeyMax;
+          const bool none = key == kKeyMax;
+          oi[t] = none ? -1 : key_idx(key);
+          const float d2 = key_d2(key);
+          od[t] = none ? __int_as_float(0x7f800000) : (a.squared ? d2 : sqrtf(d2));
+        }
+      }
+      __syncwarp();
+    }
+    TILE_PROF(6);
+    __syncthreads();  // the next tile overwrites the query tile and centre
+    TILE_PROF(7);
+  }
+  if (!ok && tid == 0) atomicExch(a.err, 1);
+#if KNN_TILE_PROFILE
+  if (tid == 0)
+    for (int i = 0; i < 8; i++) atomicAdd(&tile_prof[i], prof[i]);
+#endif
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(kFull, pairs, o);
+  if (lane == 0) {
+    atomicAdd(&a.counters[0], pairs);
+    atomicAdd(&a.counters[1], refined);
+    atomicAdd(&a.counters[2], rechecks);
+    atomicAdd(&a.counters[3], fallbacks);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, kTN);
+}
+
+int pow2_at_least(int v) {
+  int p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+}  // namespace
+
+bool tile_search_supported(int d, int k, int margin) {
+  return d >= 16 && d <= 256 && k >= 1 && k <= KNN_MAX_K && margin >= 0 && margin <= 4096;
+}
+
+// Shared memory of one CTA for a per-query buffer of `cap` entries.
+static size_t tile_smem_bytes(int KD, int cap) {
+  return tc::tile_bytes(kTM, KD) + tc::tile_bytes(kTN, KD) + (size_t)KD * 4 +
+         (size_t)kTN * 16 + 11 * (size_t)kTN * 4 + (4 + 4) * 4 + 4 * 256 * 4 + 8 + 4 + 16 + 16 +
+         4 * (size_t)cap * 12;
+}
+
+int tile_search_geometry(int d, int k, int margin, int num_sms, int *grid, int *cap, int *P,
+                         size_t *smem) {
+  const int KD = std::max(16, pow2_at_least(d));
+  *P = std::max(32, pow2_at_least(k + 64));
+  // each query keeps up to cap bound pairs; smaller if shared memory is short
+  *cap = 4 * (k + margin) + kTN;
+  if (tile_smem_bytes(KD, *cap) > 227 * 1024) *cap = 2 * (k + margin) + kTN;
+  *cap = std::max(*cap, *P);
+  // at least 48 KB: no more than four CTAs (4 x 128 TMEM columns) per SM
+  *smem = std::max<size_t>(tile_smem_bytes(KD, *cap), 48 * 1024 + 1024);
+  if (*smem > 227 * 1024) return KNN_EINVAL;
+  KNN_CUDA_TRY(cudaFuncSetAttribute(tile_search_kernel,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+  int per_sm = 0;
+  KNN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_search_kernel, kTM,
+                                                             *smem));
+  per_sm = std::max(1, std::min(per_sm, 4));
+  *grid = num_sms * per_sm;
+  return KNN_OK;
+}
+
+int launch_tile_list(const int32_t *qoff, int Rq, int32_t *tiles, int32_t *ntiles,
+                     cudaStream_t s) {
+  tile_list_kernel<<<1, 1024, 0, s>>>(qoff, Rq, tiles, ntiles);
+  KNN_LAUNCH_CHECK();
+  return KNN_OK;
+}
+
+int launch_tile_search(const TileArgs &a, int grid, size_t smem, cudaStream_t s) {
+  tile_search_kernel<<<grid, kTM, smem, s>>>(a);
+  KNN_LAUNCH_CHECK();
+  return KNN_OK;
+}
+
+}  // namespace knnsweet
+
+#if KNN_TILE_PROFILE
+// Profiling hook: copies and clears the phase timers (8 counters) and the
+// pruning counters (8 more).
+extern "C" int knnsweet_tile_profile(unsigned long long *out) {
+  if (cudaMemcpyFromSymbol(out, knnsweet::tile_prof, 16 * sizeof(unsigned long long)) !=
+      cudaSuccess)
+    return -3;
+  unsigned long long z[16] = {};
+  return cudaMemcpyToSymbol(knnsweet::tile_prof, z, sizeof z) == cudaSuccess ? 0 : -3;
+}
+#endif

@@ -1,0 +1,169 @@
+// warp_select.cuh -- warp-level helpers on 64-bit (distance, index) keys
+// shared by the pruned scan and the tensor-core tile search: 64-bit
+// shuffles, the exact k-th key by radix selection, and a runtime-length
+// bitonic sort in shared memory.
+#pragma once
+
+#include "common.cuh"
+
+namespace knnsweet {
+
+__device__ __forceinline__ uint64_t shfl_xor64(uint64_t v, int m) {
+  uint32_t lo = __shfl_xor_sync(kFull, (uint32_t)v, m);
+  uint32_t hi = __shfl_xor_sync(kFull, (uint32_t)(v >> 32), m);
+  return ((uint64_t)hi << 32) | lo;
+}
+__device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) {
+  uint32_t lo = __shfl_sync(kFull, (uint32_t)v, src);
+  uint32_t hi = __shfl_sync(kFull, (uint32_t)(v >> 32), src);
+  return ((uint64_t)hi << 32) | lo;
+}
+__device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+__device__ __forceinline__ uint64_t umax64(uint64_t a, uint64_t b) { return a < b ? b : a; }
+
+// k-th smallest (1-based rank k, 1 <= k <= n) of the distinct keys s[0..n),
+// by one warp: radix selection with 8-bit digits, starting at the highest bit
+// in which the keys differ; `hist` is a 256-word shared-memory histogram.
+// (Inlined: an out-of-line call spilled the caller's registers around it.)
+__device__ __forceinline__ uint64_t warp_select_kth(const uint64_t *s, int n, int k,
+                                                 uint32_t *hist, int lane) {
+  uint64_t mn = kKeyMax, mx = 0;
+  for (int i = lane; i < n; i += 32) {
+    const uint64_t v = s[i];
+    mn = umin64(mn, v);
+    mx = umax64(mx, v);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = umin64(mn, shfl_xor64(mn, o));
+    mx = umax64(mx, shfl_xor64(mx, o));
+  }
+  if (mn == mx) return mn;
+  const int hb = 63 - __clzll((long long)(mn ^ mx));  // highest differing bit
+  uint64_t known = hb == 63 ? 0ull : (~0ull << (hb + 1));
+  uint64_t prefix = mn & known;
+  uint32_t need = (uint32_t)k;
+  int top = hb + 1;  // bits [0, top) still unknown
+  for (;;) {
+    const int shift = top > 8 ? top - 8 : 0;
+    const uint32_t dmask = (1u << (top - shift)) - 1u;
+    __syncwarp();
+#pragma unroll
+    for (int b = 0; b < 8; b++) hist[b * 32 + lane] = 0;
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) {
+      const uint64_t v = s[i];
+      if ((v & known) == prefix) atomicAdd(&hist[(uint32_t)(v >> shift) & dmask], 1u);
+    }
+    __syncwarp();
+    // bin holding the need-th key: scan the bins 32 at a time
+    uint32_t base = 0, before = 0, cnt_b = 0;
+    int bin = -1;
+#pragma unroll 1
+    for (int j = 0; j < 8 && bin < 0; j++) {
+      const uint32_t h = hist[j * 32 + lane];
+      uint32_t incl = h;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+      }
+      const uint32_t total = __shfl_sync(kFull, incl, 31);
+      if (base + total >= need) {
+        const int wl = __ffs(__ballot_sync(kFull, base + incl >= need)) - 1;
+        bin = j * 32 + wl;
+        before = base + __shfl_sync(kFull, incl - h, wl);
+        cnt_b = __shfl_sync(kFull, h, wl);
+      }
+      base += total;
+    }
+    need -= before;
+    prefix |= (uint64_t)bin << shift;
+    known |= (uint64_t)dmask << shift;
+    if (shift == 0) return prefix;
+    if (cnt_b == 1) {  // the only key with this prefix
+      uint64_t found = 0;
+      bool f = false;
+      for (int i = lane; i < n; i += 32) {
+        const uint64_t v = s[i];
+        if ((v & known) == prefix) {
+          found = v;
+          f = true;
+        }
+      }
+      return shfl64(found, __ffs(__ballot_sync(kFull, f)) - 1);
+    }
+    top = shift;
+  }
+}
+
+// k-th smallest (1-based, 1 <= k <= n) of the 32-bit values s[i * stride],
+// i < n, which may repeat: the value v with #{s < v} < k <= #{s <= v}.  One
+// warp, four 8-bit digit passes over s (global or shared memory); `hist` is
+// a 256-word shared-memory histogram.  Non-negative floats order like their
+// bit patterns, so this also selects among non-negative floats.
+__device__ __forceinline__ uint32_t warp_select_kth_u32(const uint32_t *s, int stride, int n,
+                                                        int k, uint32_t *hist, int lane) {
+  uint32_t prefix = 0, known = 0, need = (uint32_t)k;
+#pragma unroll 1
+  for (int shift = 24; shift >= 0; shift -= 8) {
+    __syncwarp();
+#pragma unroll
+    for (int b = 0; b < 8; b++) hist[b * 32 + lane] = 0;
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) {
+      const uint32_t v = s[(size_t)i * stride];
+      if ((v & known) == prefix) atomicAdd(&hist[(v >> shift) & 255u], 1u);
+    }
+    __syncwarp();
+    uint32_t base = 0, before = 0;
+    int bin = -1;
+#pragma unroll 1
+    for (int j = 0; j < 8 && bin < 0; j++) {
+      const uint32_t h = hist[j * 32 + lane];
+      uint32_t incl = h;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+      }
+      const uint32_t total = __shfl_sync(kFull, incl, 31);
+      if (base + total >= need) {
+        const int wl = __ffs(__ballot_sync(kFull, base + incl >= need)) - 1;
+        bin = j * 32 + wl;
+        before = base + __shfl_sync(kFull, incl - h, wl);
+      }
+      base += total;
+    }
+    need -= before;
+    prefix |= (uint32_t)bin << shift;
+    known |= 255u << shift;
+  }
+  __syncwarp();
+  return prefix;
+}
+
+// Bitonic sort of n keys in shared memory (n a power of two), ascending, by
+// one warp.
+__device__ __forceinline__ void smem_bitonic_sort_rt(uint64_t *s, int n, int lane) {
+#pragma unroll 1
+  for (int size = 2; size <= n; size <<= 1) {
+#pragma unroll 1
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+#pragma unroll 1
+      for (int t = lane; t < n / 2; t += 32) {
+        const int i = 2 * t - (t & (stride - 1));
+        const int j = i + stride;
+        const bool up = (i & size) == 0;
+        const uint64_t a = s[i], b = s[j];
+        if ((a > b) == up) {
+          s[i] = b;
+          s[j] = a;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+}  // namespace knnsweet

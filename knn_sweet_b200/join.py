@@ -39,7 +39,7 @@ class JoinStats:
     qreps_used: int
     sreps_used: int
     kernels_launched: int
-    reserved: int = 0
+    refine_fallbacks: int = 0
 
 
 def _options(qreps, sreps, seed, rep_trials, precision, margin,
