@@ -211,9 +211,13 @@ int build_clusters(Arena &ar, const float4 *rows, int64_t n, int d, int dp4s, in
   // nearest representative (BF16 tensor-core arg-min + exact FP32 distance to
   // the winner for d >= 16, FP32 CUDA cores otherwise), then one sort into
   // clusters; with Lloyd steps the representatives move to their clusters'
-  // centroids and the points are assigned and sorted again
+  // centroids (the smallest clusters' representatives to the farthest member
+  // of the widest clusters) and the points are assigned and sorted again
   for (int it = 0; it <= lloyd_iters; it++) {
-    if (it > 0) KNN_TRY(launch_centroids(rows, dp4s, cs->perm, cs->off, R, cs->reps, s));
+    if (it > 0) {
+      KNN_TRY(launch_centroids(rows, dp4s, cs->perm, cs->off, R, cs->reps, s));
+      KNN_TRY(launch_split_clusters(rows, dp4s, cs->perm, cs->off, cs->skeys, R, cs->reps, s));
+    }
     if (tc_assign)
       KNN_TRY(launch_assign_tc(rows, n, dp4s, d, cs->reps, R, tc_scratch, cl, dr, err, s));
     else

@@ -11,6 +11,8 @@
 //   rep_dist_kernel        representative-to-representative distances
 //   bounds_filter_kernel   per query cluster: k-th upper bound + surviving
 //                          reference clusters sorted by rep-rep distance
+#include <algorithm>
+
 #include <cub/device/device_radix_sort.cuh>
 
 #include "bounds.cuh"
@@ -263,6 +265,87 @@ __global__ void __launch_bounds__(256)
 int launch_centroids(const float4 *rows, int dp4, const int32_t *perm, const int32_t *off, int R,
                      float4 *reps, cudaStream_t s) {
   centroid_kernel<<<R, 256, 0, s>>>(rows, dp4, perm, off, reps);
+  KNN_LAUNCH_CHECK();
+  return KNN_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Cluster split (refinement steps only; the reference has no counterpart).
+// A random draw leaves some dense regions without a representative; their
+// points join a distant cluster whose radius then spans both regions, and
+// such clusters defeat the triangle-inequality bounds.  Each refinement step
+// pairs the smallest clusters (donors) with the widest ones (receivers) and
+// moves each donor's representative onto its receiver's farthest member, so
+// the next assignment splits the receiver.  A pair moves only when the
+// receiver's radius is more than twice the median radius and the donor holds
+// fewer points than the median cluster.  Deterministic: both orders break
+// ties by cluster id.  One block; R <= 8192.
+// dynamic shared memory: 2 * pow2(R) keys
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024)
+    split_clusters_kernel(const float4 *__restrict__ rows, int dp4,
+                          const int32_t *__restrict__ perm, const int32_t *__restrict__ off,
+                          const uint64_t *__restrict__ skeys, int R, int rp2, int max_moves,
+                          float4 *__restrict__ reps) {
+  extern __shared__ uint64_t sk[];
+  uint64_t *by_size = sk, *by_radius = sk + rp2;
+  const int tid = threadIdx.x;
+  for (int c = tid; c < rp2; c += blockDim.x) {
+    uint64_t ks = kKeyMax, kr = kKeyMax;
+    if (c < R) {
+      const int a = off[c], b = off[c + 1];
+      const float rad = b > a ? __uint_as_float((uint32_t)skeys[b - 1]) : 0.0f;
+      ks = ((uint64_t)(uint32_t)(b - a) << 32) | (uint32_t)c;
+      kr = ((uint64_t)(~__float_as_uint(rad)) << 32) | (uint32_t)c;  // widest first
+    }
+    by_size[c] = ks;
+    by_radius[c] = kr;
+  }
+  __syncthreads();
+  for (int size = 2; size <= rp2; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int t = tid; t < rp2 / 2; t += blockDim.x) {
+        const int i = 2 * t - (t & (stride - 1)), j = i + stride;
+        const bool up = (i & size) == 0;
+        uint64_t x = by_size[i], y = by_size[j];
+        if ((x > y) == up) {
+          by_size[i] = y;
+          by_size[j] = x;
+        }
+        x = by_radius[i];
+        y = by_radius[j];
+        if ((x > y) == up) {
+          by_radius[i] = y;
+          by_radius[j] = x;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  const float med_rad = __uint_as_float(~(uint32_t)(by_radius[R / 2] >> 32));
+  const uint32_t med_size = (uint32_t)(by_size[R / 2] >> 32);
+  for (int i = tid; i < max_moves; i += blockDim.x) {
+    const int recv = (int)(uint32_t)by_radius[i];
+    const int donor = (int)(uint32_t)by_size[i];
+    const float rad = __uint_as_float(~(uint32_t)(by_radius[i] >> 32));
+    const uint32_t dsize = (uint32_t)(by_size[i] >> 32);
+    if (recv == donor || !(rad > 2.0f * med_rad) || dsize >= med_size) continue;
+    const int far = perm[off[recv + 1] - 1];
+    for (int ch = 0; ch < dp4; ch++) reps[(int64_t)donor * dp4 + ch] = rows[(int64_t)far * dp4 + ch];
+  }
+}
+
+int launch_split_clusters(const float4 *rows, int dp4, const int32_t *perm, const int32_t *off,
+                          const uint64_t *skeys, int R, float4 *reps, cudaStream_t s) {
+  if (R < 4) return KNN_OK;
+  int rp2 = 1;
+  while (rp2 < R) rp2 <<= 1;
+  const size_t smem = 2 * (size_t)rp2 * sizeof(uint64_t);
+  if (smem > 48 * 1024)
+    KNN_CUDA_TRY(cudaFuncSetAttribute(split_clusters_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  split_clusters_kernel<<<1, 1024, smem, s>>>(rows, dp4, perm, off, skeys, R, rp2,
+                                              std::max(1, R / 16), reps);
   KNN_LAUNCH_CHECK();
   return KNN_OK;
 }

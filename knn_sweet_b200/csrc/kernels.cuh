@@ -52,6 +52,8 @@ int launch_assign_tc(const float4 *rows, int64_t n, int dp4, int d, const float4
 size_t cluster_sort_temp_bytes(int64_t n, int R);
 int launch_centroids(const float4 *rows, int dp4, const int32_t *perm, const int32_t *off, int R,
                      float4 *reps, cudaStream_t s);
+int launch_split_clusters(const float4 *rows, int dp4, const int32_t *perm, const int32_t *off,
+                          const uint64_t *skeys, int R, float4 *reps, cudaStream_t s);
 int launch_cluster_sort(const int32_t *cl, const float *dr, int64_t n, int R,
                         uint64_t *keys, int32_t *vals, uint64_t *skeys,
                         int32_t *perm, void *temp, size_t temp_bytes,

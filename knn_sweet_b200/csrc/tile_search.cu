@@ -121,39 +121,56 @@ __device__ __forceinline__ void stage_tile(unsigned char *tile, const float *sc,
                                            int dp4, RowPtr rowptr, float *o_n, float *o_e,
                                            float *o_t) {
   const int G = KD >> 3;
-  for (int t = threadIdx.x; t < kTM * G; t += kTM) {
-    const int r = t / G, g = t - r * G, k0 = g << 3;
-    const float4 *row = rowptr(r);
-    float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f), c1 = c0;
-    if (row) {
-      if ((k0 >> 2) < dp4) c0 = row[k0 >> 2];
-      if ((k0 >> 2) + 1 < dp4) c1 = row[(k0 >> 2) + 1];
-    }
-    const float v[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-    float sn = 0.0f, se = 0.0f, st = 0.0f;
-    __align__(16) __nv_bfloat16 h[8];
+  // four 16-byte groups per thread per round, their loads issued together
+  // (whether a round's group exists depends only on the round: uniform)
+  for (int t0 = threadIdx.x; t0 < kTM * G; t0 += 4 * kTM) {
+    float4 c0[4], c1[4];
+    bool has[4];
 #pragma unroll
-    for (int e = 0; e < 8; e++) {
-      const int kk = k0 + e;
-      const float x = (row && kk < d) ? __fsub_rn(v[e], sc[kk]) : 0.0f;
-      h[e] = __float2bfloat16_rn(x);
-      const float xr = __bfloat162float(h[e]);
-      const float df = __fsub_rn(x, xr);
-      sn = __fmaf_rn(x, x, sn);
-      se = __fmaf_rn(df, df, se);
-      st = __fmaf_rn(xr, xr, st);
+    for (int u = 0; u < 4; u++) {
+      const int t = t0 + u * kTM;
+      const int r = t / G, k0 = (t - r * G) << 3;
+      const float4 *row = t < kTM * G ? rowptr(r) : nullptr;
+      has[u] = row != nullptr;
+      c0[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+      c1[u] = c0[u];
+      if (row) {
+        if ((k0 >> 2) < dp4) c0[u] = row[k0 >> 2];
+        if ((k0 >> 2) + 1 < dp4) c1[u] = row[(k0 >> 2) + 1];
+      }
     }
-    *reinterpret_cast<uint4 *>(tile + tc::tile_offset(r, k0, KD)) =
-        *reinterpret_cast<const uint4 *>(h);
-    for (int o = G >> 1; o > 0; o >>= 1) {
-      sn += __shfl_xor_sync(kFull, sn, o);
-      se += __shfl_xor_sync(kFull, se, o);
-      st += __shfl_xor_sync(kFull, st, o);
-    }
-    if (g == 0) {
-      o_n[r] = sn;
-      o_e[r] = se;
-      o_t[r] = st;
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int t = t0 + u * kTM;
+      if (t >= kTM * G) break;
+      const int r = t / G, g = t - r * G, k0 = g << 3;
+      const float v[8] = {c0[u].x, c0[u].y, c0[u].z, c0[u].w,
+                          c1[u].x, c1[u].y, c1[u].z, c1[u].w};
+      float sn = 0.0f, se = 0.0f, st = 0.0f;
+      __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int kk = k0 + e;
+        const float x = (has[u] && kk < d) ? __fsub_rn(v[e], sc[kk]) : 0.0f;
+        h[e] = __float2bfloat16_rn(x);
+        const float xr = __bfloat162float(h[e]);
+        const float df = __fsub_rn(x, xr);
+        sn = __fmaf_rn(x, x, sn);
+        se = __fmaf_rn(df, df, se);
+        st = __fmaf_rn(xr, xr, st);
+      }
+      *reinterpret_cast<uint4 *>(tile + tc::tile_offset(r, k0, KD)) =
+          *reinterpret_cast<const uint4 *>(h);
+      for (int o = G >> 1; o > 0; o >>= 1) {
+        sn += __shfl_xor_sync(kFull, sn, o);
+        se += __shfl_xor_sync(kFull, se, o);
+        st += __shfl_xor_sync(kFull, st, o);
+      }
+      if (g == 0) {
+        o_n[r] = sn;
+        o_e[r] = se;
+        o_t[r] = st;
+      }
     }
   }
 }
@@ -201,13 +218,27 @@ __device__ __forceinline__ void copy_entries(float2 *dlu, int32_t *dpos, const f
 }
 
 // Exact squared distance in FP32 over the first d columns, in column order:
-// the value the FP32 scan computes for the same pair.
-__device__ __forceinline__ float dist2_cols(const float *__restrict__ q,
-                                            const float *__restrict__ r, int d) {
+// the value the FP32 scan computes for the same pair (padding columns add
+// exact zeros there).  Rows are float4-aligned.
+__device__ __forceinline__ float dist2_cols(const float4 *__restrict__ q,
+                                            const float4 *__restrict__ r, int d) {
   float acc = 0.0f;
-  for (int c = 0; c < d; c++) {
-    const float t = __fsub_rn(q[c], r[c]);
-    acc = __fmaf_rn(t, t, acc);
+  const int full = d >> 2;
+  for (int c = 0; c < full; c++) {
+    const float4 u = q[c], v = r[c];
+    float t;
+    t = __fsub_rn(u.x, v.x); acc = __fmaf_rn(t, t, acc);
+    t = __fsub_rn(u.y, v.y); acc = __fmaf_rn(t, t, acc);
+    t = __fsub_rn(u.z, v.z); acc = __fmaf_rn(t, t, acc);
+    t = __fsub_rn(u.w, v.w); acc = __fmaf_rn(t, t, acc);
+  }
+  const int rem = d & 3;
+  if (rem) {
+    const float4 u = q[full], v = r[full];
+    float t;
+    t = __fsub_rn(u.x, v.x); acc = __fmaf_rn(t, t, acc);
+    if (rem > 1) { t = __fsub_rn(u.y, v.y); acc = __fmaf_rn(t, t, acc); }
+    if (rem > 2) { t = __fsub_rn(u.z, v.z); acc = __fmaf_rn(t, t, acc); }
   }
   return acc;
 }
@@ -257,7 +288,8 @@ __global__ void __launch_bounds__(kTM)
   // per warp: one query's buffer (cap bound pairs, cap positions)
   const size_t wofs = ((size_t)(reinterpret_cast<unsigned char *>(s_tile + 4) - smem) + 15) &
                       ~(size_t)15;
-  unsigned char *wbase = smem + wofs + (size_t)warp * cap * 12;
+  float4 *wq = reinterpret_cast<float4 *>(smem + wofs) + (size_t)warp * dp4;
+  unsigned char *wbase = smem + wofs + 4 * (size_t)dp4 * 16 + (size_t)warp * cap * 12;
   float2 *w_lu = reinterpret_cast<float2 *>(wbase);
   int32_t *w_pos = reinterpret_cast<int32_t *>(wbase + (size_t)cap * 8);
   uint32_t *whist = hist + warp * 256;
@@ -340,8 +372,44 @@ __global__ void __launch_bounds__(kTM)
     //     its members with d(s,Rc) in [dl - theta_q, du + theta_q]
     //     (triangle inequality), one contiguous run of the sorted members.
     // The tile streams, per cluster, the union of its queries' runs.
-    for (int jb = 0; jb < nl && ok; jb += kTN) {
-      const int nb = min(kTN, nl - jb);
+    // compacts every buffer of the tile holding more than `above` pairs (and
+    // at least k); the rows are shared out over the four warps through shared
+    // memory.  Called by the whole CTA.
+    int *s_req = reinterpret_cast<int *>(s_n);
+    int *s_kept = reinterpret_cast<int *>(s_e);
+    float *s_uk = s_t;
+    auto compact_rows = [&](int above) {
+      const bool mine = valid && !ovf && n > above && n >= k;
+      s_req[tid] = mine ? n : 0;
+      if (!__syncthreads_or(mine)) return;
+      for (int rr = warp; rr < cnt; rr += 4) {
+        const int nn = s_req[rr];
+        if (nn == 0) continue;
+        const size_t ro = (row0 + rr) * cap;
+        float uk;
+        copy_entries(w_lu, w_pos, a.buf_lu + ro, a.buf_pos + ro, nn, lane);
+        const int kept = compact_bounds(w_lu, w_pos, nn, k, whist, lane, &uk);
+        copy_entries(a.buf_lu + ro, a.buf_pos + ro, w_lu, w_pos, kept, lane);
+        if (lane == 0) {
+          s_kept[rr] = kept;
+          s_uk[rr] = uk;
+        }
+      }
+      __syncthreads();
+      if (mine) {
+        const int kept = s_kept[tid];
+        const float uk = s_uk[tid];
+        n = kept;
+        tau = fminf(tau, uk);
+        th_q = fminf(th_q, sqrtf(uk) * (1.0f + tol));
+        lim = min(cap - kTN, 2 * kept + 32);
+        if (kept > cap - kTN) ovf = true;
+      }
+    };
+    // the first batch holds the four nearest clusters only: they tighten the
+    // bounds before the rest of the list is decided
+    for (int jb = 0, nb = 0; jb < nl && ok; jb += nb) {
+      nb = jb == 0 ? min(4, nl) : min(kTN, nl - jb);
       stage_tile(
           sb, sc, KD, d, dp4,
           [&](int r) -> const float4 * {
@@ -471,6 +539,7 @@ __global__ void __launch_bounds__(kTM)
       // the runs, concatenated, in chunks of kTN rows
       for (int o = 0; o < total; o += kTN) {
         const int nr = min(kTN, total - o);
+        const bool last_of_first = jb == 0 && o + kTN >= total;
         stage_tile(
             sb, sc, KD, d, dp4,
             [&](int r) -> const float4 * {
@@ -532,24 +601,10 @@ __global__ void __launch_bounds__(kTM)
         }
         if (valid) pairs += (unsigned long long)nr;
         TILE_PROF(3);
-        // buffers past their limit are compacted (tightening tau)
-        unsigned need = __ballot_sync(kFull, valid && !ovf && n > lim);
-        while (need) {
-          const int rr = __ffs(need) - 1;
-          need &= need - 1u;
-          const int nn = __shfl_sync(kFull, n, rr);
-          const size_t ro = (row0 + warp * 32 + rr) * cap;
-          float uk;
-          copy_entries(w_lu, w_pos, a.buf_lu + ro, a.buf_pos + ro, nn, lane);
-          const int kept = compact_bounds(w_lu, w_pos, nn, k, whist, lane, &uk);
-          copy_entries(a.buf_lu + ro, a.buf_pos + ro, w_lu, w_pos, kept, lane);
-          if (lane == rr) {
-            n = kept;
-            tau = fminf(tau, uk);
-            lim = min(cap - kTN, 2 * kept + 32);
-            if (kept > cap - kTN) ovf = true;
-          }
-        }
+        // buffers past their limit are compacted (tightening tau); after the
+        // first batch every buffer holding k pairs is, so that the next
+        // batch's runs use the tightened bounds
+        compact_rows(last_of_first ? k - 1 : lim);
         TILE_PROF(4);
         tc::fence_before_sync();
         __syncthreads();  // the member tile, TMEM and column scalars are reused
@@ -566,13 +621,15 @@ __global__ void __launch_bounds__(kTM)
       atomicAdd(&tile_prof[15], 1ull);
     }
 #endif
-    // finish this warp's queries: exact re-ranking and the FP64 boundary,
-    // on a shared-memory copy of each query's buffer
-    for (int i = 0; i < 32; i++) {
-      const int row = warp * 32 + i;
-      if (row >= cnt) break;
-      const int nn = __shfl_sync(kFull, n, i);
-      bool fb = __shfl_sync(kFull, (int)ovf, i) != 0;
+    // finish the tile's queries, shared out over the four warps: exact
+    // re-ranking and the FP64 boundary, on a shared-memory copy of each
+    // query's buffer
+    s_req[tid] = n;
+    s_kept[tid] = ovf ? 1 : 0;
+    __syncthreads();
+    for (int row = warp; row < cnt; row += 4) {
+      const int nn = s_req[row];
+      bool fb = s_kept[row] != 0;
       const int slot = s0 + row;
       const int64_t q = a.qorder[slot];
       const size_t ro = (row0 + row) * cap;
@@ -587,11 +644,12 @@ __global__ void __launch_bounds__(kTM)
       // exact FP32 keys, written over the bound pairs
       uint64_t *keys = reinterpret_cast<uint64_t *>(w_lu);
       const float *qf = reinterpret_cast<const float *>(a.qrows + (size_t)q * dp4);
+      for (int c = lane; c < dp4; c += 32) wq[c] = a.qrows[(size_t)q * dp4 + c];
+      __syncwarp();
       if (!fb) {
         for (int e = lane; e < m1; e += 32) {
           const int p = w_pos[e];
-          const float d2 =
-              dist2_cols(qf, reinterpret_cast<const float *>(a.srows + (size_t)p * dp4), d);
+          const float d2 = dist2_cols(wq, a.srows + (size_t)p * dp4, d);
           keys[e] = make_key(d2, a.sidx[p]);
         }
         if (lane == 0) refined += (unsigned long long)m1;
@@ -720,7 +778,7 @@ bool tile_search_supported(int d, int k, int margin) {
 static size_t tile_smem_bytes(int KD, int cap) {
   return tc::tile_bytes(kTM, KD) + tc::tile_bytes(kTN, KD) + (size_t)KD * 4 +
          (size_t)kTN * 16 + 11 * (size_t)kTN * 4 + (4 + 4) * 4 + 4 * 256 * 4 + 8 + 4 + 16 + 16 +
-         4 * (size_t)cap * 12;
+         4 * (size_t)cap * 12 + 4 * (size_t)(KD / 4) * 16;
 }
 
 int tile_search_geometry(int d, int k, int margin, int num_sms, int *grid, int *cap, int *P,
