@@ -47,6 +47,8 @@ def parse_args(argv=None):
     ap.add_argument("--n", type=int, default=245_057, help="points (default: full size)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the BF16+refine and batched form comparisons")
     return ap.parse_args(argv)
 
 
@@ -339,6 +341,8 @@ def run_ours(args):
     }
     if e2e:
         line["e2e"] = e2e
+    if world == 1 and not args.no_forms:
+        line["forms"] = run_forms(torch, dev, flush)
     if world == 1 and not args.no_cpu_baseline:
         cores = host_cores()
         sample = cpu_sample_size(x, cores, 10.0)
@@ -351,6 +355,88 @@ def run_ours(args):
     if pg:
         pg.destroy_process_group()
     return 0
+
+
+def _time_steps(torch, dev, fn, steps, flush):
+    """Mean device time (ms) of `steps` calls of fn, L2 flushed before each."""
+    fn()
+    torch.cuda.synchronize(dev)
+    ms = []
+    for i in range(steps):
+        flush.fill_(i & 0xFF)
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        fn()
+        s1.record()
+        torch.cuda.synchronize(dev)
+        ms.append(s0.elapsed_time(s1))
+    return statistics.mean(ms)
+
+
+def run_forms(torch, dev, flush, steps=3):
+    """The precision and batching forms beside the plain FP32 join.
+
+    precision: 2,000,000 reference / 200,000 query points, d=128, k=100
+    (seeded mixture of 4,096 Gaussians), plain FP32 vs BF16+refine on the same
+    representatives; neighbour-set agreement between the two forms.
+    batching: 4,096 ellipsoid clouds of 256..16,384 points, d=3, per-cloud
+    self-join k=16: one graph-replayed batched call vs one plain call per cloud.
+    """
+    import knn_sweet_b200 as ks
+    from knn_sweet_b200 import data
+    from knn_sweet_b200.batched import BatchedJoinGraph
+    out = {}
+    r, q = data.config3()
+    rt, qt = torch.from_numpy(r).to(dev), torch.from_numpy(q).to(dev)
+    del r, q
+    m, k = qt.shape[0], 100
+    kw = dict(qreps=8192, sreps=8192, lloyd_iters=4)
+    res, forms = {}, {}
+    for prec in ("fp32", "bf16_refine"):
+        o = (torch.empty((m, k), dtype=torch.int32, device=dev),
+             torch.empty((m, k), dtype=torch.float32, device=dev))
+        ms = _time_steps(torch, dev, lambda: ks.knnjoin(qt, rt, k, precision=prec, out=o, **kw),
+                         steps, flush)
+        _, _, st = ks.knnjoin(qt, rt, k, precision=prec, out=o, stats=True, **kw)
+        res[prec] = o
+        forms[prec] = {"queries_per_s": m / (ms * 1e-3), "ms_per_step": ms,
+                       "build_ms": st.ms_build, "search_ms": st.ms_search,
+                       "dist_evals_per_query": st.dist_evals / m,
+                       "fp64_rechecks": st.refine_rechecks,
+                       "fallback_queries": st.refine_fallbacks}
+    a, b = res["fp32"][0], res["bf16_refine"][0]
+    same = (torch.sort(a, 1)[0] == torch.sort(b, 1)[0]).all(1).float().mean().item()
+    out["precision"] = {
+        "workload": f"N=2,000,000 M={m} d=128 k={k} reps 8192/8192 lloyd 4, synthetic "
+                    "4,096-Gaussian mixture", "fp32": forms["fp32"],
+        "bf16_refine": forms["bf16_refine"], "same_neighbor_sets": same,
+        "bf16_over_fp32": forms["bf16_refine"]["queries_per_s"] / forms["fp32"]["queries_per_s"]}
+    del rt, qt, res, a, b
+
+    pts, off = data.ellipsoid_clouds()
+    x = torch.from_numpy(pts).to(dev)
+    mq, kb = x.shape[0], 16
+    g = BatchedJoinGraph(off, d=3, k=kb)
+    g(x)
+    torch.cuda.synchronize(dev)
+    ms_b = _time_steps(torch, dev, lambda: g(x), steps, flush)
+    bi, bd = g.idx.clone(), g.dist.clone()
+    oi = torch.empty((mq, kb), dtype=torch.int32, device=dev)
+    od = torch.empty((mq, kb), dtype=torch.float32, device=dev)
+    bounds = [(int(off[c]), int(off[c + 1])) for c in range(len(off) - 1)]
+
+    def per_cloud():
+        for a0, a1 in bounds:
+            ks.knnjoin(x[a0:a1], None, kb, out=(oi[a0:a1], od[a0:a1]))
+    ms_p = _time_steps(torch, dev, per_cloud, 1, flush)
+    same_b = (torch.sort(oi, 1)[0] == torch.sort(bi, 1)[0]).all(1).float().mean().item()
+    out["batching"] = {
+        "workload": f"{len(bounds)} ellipsoid clouds, {mq} points, d=3, per-cloud self-join "
+                    f"k={kb}", "batched_graph": {"queries_per_s": mq / (ms_b * 1e-3),
+                                                 "ms_per_step": ms_b},
+        "per_cloud_calls": {"queries_per_s": mq / (ms_p * 1e-3), "ms_per_step": ms_p},
+        "same_neighbor_sets": same_b, "batched_over_per_cloud": ms_p / ms_b}
+    return out
 
 
 def main(argv=None):
