@@ -298,9 +298,30 @@ struct EventSet {
   }
 };
 
+// Host destination of the result for the host-buffer entry point: the scan
+// then runs in row chunks and each chunk's rows are copied back on `copy`
+// while the next chunk is computed.  `done` tells whether the copies were
+// enqueued (otherwise the caller copies the whole result).
+struct HostSink {
+  int32_t *idx;
+  float *dist;
+  cudaStream_t copy;
+  bool done;
+};
+
+// Events of the chunked copies, destroyed once both streams are idle.
+struct ChunkEvents {
+  std::vector<cudaEvent_t> ev;
+  ~ChunkEvents() {
+    for (auto e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
 int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
                      int32_t d, int32_t k, int32_t *out_idx, float *out_dist,
-                     const knn_options *opt, knn_stats *st, cudaStream_t s) {
+                     const knn_options *opt, knn_stats *st, cudaStream_t s,
+                     HostSink *sink = nullptr) {
   knn_options o;
   KNN_TRY(check_options(opt, &o));
   KNN_TRY(check_sizes(m, n, d, k));
@@ -493,13 +514,63 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
     a.slot_list = fb_slots;
     a.slot_count = fb_count;
   }
-  KNN_TRY(launch_scan(a, num_sms, s));
+  // host destination and a large result: scan in row chunks (each chunk's
+  // slots still in query-cluster order) and copy every finished chunk back
+  // while the next one runs
+  const int64_t out_bytes = m * (int64_t)k * 8;
+  const int nchunks = (sink && !tiles && out_bytes >= (16 << 20) && m >= 8 * 1024) ? 8 : 1;
+  ChunkEvents cev;
+  if (nchunks > 1) {
+    const int chunk_rows = (int)((m + nchunks - 1) / nchunks);
+    uint32_t *ckeys, *ckeys_out;
+    int32_t *cvals, *cslots, *ccount;
+    unsigned long long *cwork;
+    const size_t tb = chunk_slots_temp_bytes(m, nchunks);
+    unsigned char *ctemp;
+    KNN_TRY(ar.alloc(&ckeys, (size_t)m));
+    KNN_TRY(ar.alloc(&ckeys_out, (size_t)m));
+    KNN_TRY(ar.alloc(&cvals, (size_t)m));
+    KNN_TRY(ar.alloc(&cslots, (size_t)m));
+    KNN_TRY(ar.alloc(&ctemp, tb));
+    KNN_TRY(ar.alloc(&ccount, (size_t)nchunks));
+    KNN_TRY(ar.alloc(&cwork, (size_t)nchunks));
+    KNN_CUDA_TRY(cudaMemsetAsync(cwork, 0, nchunks * sizeof(unsigned long long), s));
+    std::vector<int32_t> counts(nchunks);
+    for (int c = 0; c < nchunks; c++)
+      counts[c] = (int32_t)std::max<int64_t>(0, std::min<int64_t>(chunk_rows, m - (int64_t)c * chunk_rows));
+    KNN_TRY(upload_i32(counts, ccount, s));
+    KNN_TRY(launch_chunk_slots(qset.perm, m, chunk_rows, nchunks, ckeys, ckeys_out, cvals, cslots,
+                               ctemp, tb, s));
+    cev.ev.assign(nchunks, nullptr);
+    for (int c = 0; c < nchunks; c++) {
+      if (counts[c] == 0) continue;
+      const int64_t r0 = (int64_t)c * chunk_rows;
+      ScanArgs ac = a;
+      ac.slot_list = cslots + r0;
+      ac.slot_count = reinterpret_cast<const unsigned *>(ccount + c);
+      ac.m = counts[c];
+      ac.work_counter = cwork + c;
+      KNN_TRY(launch_scan(ac, num_sms, s));
+      KNN_CUDA_TRY(cudaEventCreateWithFlags(&cev.ev[c], cudaEventDisableTiming));
+      KNN_CUDA_TRY(cudaEventRecord(cev.ev[c], s));
+      KNN_CUDA_TRY(cudaStreamWaitEvent(sink->copy, cev.ev[c], 0));
+      const size_t cnt = (size_t)counts[c] * k;
+      KNN_CUDA_TRY(cudaMemcpyAsync(sink->idx + r0 * k, out_idx + r0 * k, cnt * sizeof(int32_t),
+                                   cudaMemcpyDeviceToHost, sink->copy));
+      KNN_CUDA_TRY(cudaMemcpyAsync(sink->dist + r0 * k, out_dist + r0 * k, cnt * sizeof(float),
+                                   cudaMemcpyDeviceToHost, sink->copy));
+    }
+    sink->done = true;
+  } else {
+    KNN_TRY(launch_scan(a, num_sms, s));
+  }
   KNN_TRY(evs.record(2, s));
 
   if (st) {
     unsigned long long h[13];
     KNN_CUDA_TRY(cudaMemcpyAsync(h, ctr, sizeof h, cudaMemcpyDeviceToHost, s));
     KNN_CUDA_TRY(cudaStreamSynchronize(s));
+    if (sink && sink->done) KNN_CUDA_TRY(cudaStreamSynchronize(sink->copy));
     if (static_cast<int>(h[6] & 0xffffffffu) != 0) {
       set_error("a bounded device wait gave up (tensor-core pipeline)");
       return KNN_ETIMEOUT;
@@ -573,9 +644,16 @@ int knn_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d,
     set_error("null pointer argument");
     return KNN_EINVAL;
   }
-  cudaStream_t s;
+  cudaStream_t s, cs;
   KNN_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    cudaStreamDestroy(s);
+    set_error("stream creation failed");
+    return KNN_ECUDA;
+  }
   int rc = KNN_OK;
+  HostSink sink{out_idx, out_dist, cs, false};
   {
     Arena ar(s);
     const bool self = (q == r) && (m == n);
@@ -598,9 +676,9 @@ int knn_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d,
     if (rc == KNN_OK) {
       // always the synchronising path, which also checks the device error flag
       knn_stats local;
-      rc = join_device_impl(dq, m, dr, n, d, k, di, dd, opt, st ? st : &local, s);
+      rc = join_device_impl(dq, m, dr, n, d, k, di, dd, opt, st ? st : &local, s, &sink);
     }
-    if (rc == KNN_OK) {
+    if (rc == KNN_OK && !sink.done) {
       e = cudaMemcpyAsync(out_idx, di, sizeof(int32_t) * m * k,
                           cudaMemcpyDeviceToHost, s);
       if (e == cudaSuccess)
@@ -611,12 +689,20 @@ int knn_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d,
         rc = KNN_ECUDA;
       }
     }
+    // the result buffers are released on `s` when the arena closes: the
+    // chunk copies on `cs` must have finished by then
+    cudaError_t ec = cudaStreamSynchronize(cs);
+    if (ec != cudaSuccess && rc == KNN_OK) {
+      set_error("device-to-host copy failed: %s", cudaGetErrorString(ec));
+      rc = KNN_ECUDA;
+    }
   }
   cudaError_t e = cudaStreamSynchronize(s);
   if (e != cudaSuccess && rc == KNN_OK) {
     set_error("join failed on the device: %s", cudaGetErrorString(e));
     rc = KNN_ECUDA;
   }
+  cudaStreamDestroy(cs);
   cudaStreamDestroy(s);
   return rc;
 }

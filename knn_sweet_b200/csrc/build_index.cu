@@ -549,6 +549,43 @@ size_t cluster_sort_temp_bytes(int64_t n, int R) {
   return bytes;
 }
 
+// Query slots grouped by row chunk: chunk c holds the slots of query rows
+// [c * chunk_rows, (c + 1) * chunk_rows), in slot (query-cluster) order -- a
+// stable radix sort of the slots by chunk id.
+__global__ void chunk_keys_kernel(const int32_t *__restrict__ qorder, int64_t m, int chunk_rows,
+                                  uint32_t *__restrict__ keys, int32_t *__restrict__ vals) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    keys[i] = (uint32_t)(qorder[i] / chunk_rows);
+    vals[i] = (int32_t)i;
+  }
+}
+
+static int chunk_bits(int nchunks) {
+  int b = 1;
+  while ((1 << b) < nchunks) b++;
+  return b;
+}
+
+size_t chunk_slots_temp_bytes(int64_t m, int nchunks) {
+  size_t bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint32_t *)nullptr,
+                                  (uint32_t *)nullptr, (const int32_t *)nullptr,
+                                  (int32_t *)nullptr, (int)m, 0, chunk_bits(nchunks));
+  return bytes;
+}
+
+int launch_chunk_slots(const int32_t *qorder, int64_t m, int chunk_rows, int nchunks,
+                       uint32_t *keys, uint32_t *keys_out, int32_t *vals, int32_t *slots,
+                       void *temp, size_t temp_bytes, cudaStream_t s) {
+  chunk_keys_kernel<<<grid_for(m, 256), 256, 0, s>>>(qorder, m, chunk_rows, keys, vals);
+  KNN_LAUNCH_CHECK();
+  KNN_CUDA_TRY(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, keys_out, vals, slots,
+                                               (int)m, 0, chunk_bits(nchunks), s));
+  ++launch_counter();
+  return KNN_OK;
+}
+
 int launch_cluster_sort(const int32_t *cl, const float *dr, int64_t n, int R,
                         uint64_t *keys, int32_t *vals, uint64_t *skeys,
                         int32_t *perm, void *temp, size_t temp_bytes,

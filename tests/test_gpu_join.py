@@ -125,6 +125,22 @@ def test_deterministic_and_apis_agree(cuda_device):
         assert np.array_equal(u, v)
 
 
+@pytest.mark.parametrize("m,k", [(60000, 40), (33333, 200)])
+def test_host_path_chunked_copies_match_device_path(cuda_device, m, k):
+    """Large host-buffer joins scan in row chunks and copy each chunk back while
+    the next runs; the result must equal the device-buffer join's."""
+    x = data.skin_like(m, seed=61)
+    a = knnjoin(x, None, k)
+    b = torch_join(x, x, k)
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v)
+    r, q = data.gaussian_mix(50000, m, 8, 30, seed=62)
+    c = knnjoin(q, r, k, qreps=300, sreps=300)
+    e = torch_join(q, r, k, qreps=300, sreps=300)
+    for u, v in zip(c, e):
+        assert np.array_equal(u, v)
+
+
 def test_rep_counts_do_not_change_result(cuda_device):
     x = data.skin_like(15000, seed=51)
     base = knnjoin(x, None, 32, qreps=1, sreps=1)
