@@ -196,6 +196,9 @@ int launch_assign_tc(const float4 *rows, int64_t n, int dp4, int d, const float4
   const size_t smem = std::max<size_t>(need, 100 * 1024);
   KNN_CUDA_TRY(cudaFuncSetAttribute(assign_tc_kernel,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  KNN_CUDA_TRY(cudaFuncSetAttribute(assign_tc_kernel,
+                                    cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    cudaSharedmemCarveoutMaxShared));
   const int64_t blocks = (n + kTileM - 1) / kTileM;
   assign_tc_kernel<<<(unsigned)blocks, 128, smem, s>>>(rows, n, dp4, d, KD, tiles, rnorm,
                                                        Rpad / kTileN, cl, err);

@@ -794,9 +794,17 @@ int tile_search_geometry(int d, int k, int margin, int num_sms, int *grid, int *
   if (*smem > 227 * 1024) return KNN_EINVAL;
   KNN_CUDA_TRY(cudaFuncSetAttribute(tile_search_kernel,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
-  int per_sm = 0;
-  KNN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tile_search_kernel, kTM,
-                                                             *smem));
+  // the whole unified L1 as shared memory: the CTAs per SM are then set by
+  // shared memory alone (the default split allowed one)
+  KNN_CUDA_TRY(cudaFuncSetAttribute(tile_search_kernel,
+                                    cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    cudaSharedmemCarveoutMaxShared));
+  // CTAs per SM by shared memory (1 KB of it reserved per CTA); the
+  // persistent CTAs that find no SM slot simply start later
+  int dev = 0, smem_sm = 0;
+  KNN_CUDA_TRY(cudaGetDevice(&dev));
+  KNN_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  int per_sm = (int)((size_t)smem_sm / (*smem + 1024));
   per_sm = std::max(1, std::min(per_sm, 4));
   *grid = num_sms * per_sm;
   return KNN_OK;
