@@ -10,13 +10,14 @@
 // bounds need the exact distance to whichever representative is chosen, and
 // that distance is recomputed in FP32 afterwards (exact_rep_dist_kernel).
 //
-// One CTA (one warpgroup, 128 threads) owns 128 points: it converts them to
-// BF16 into shared memory in the core-matrix layout of tc_common.cuh, then for
-// every tile of 256 representatives (pre-converted once) thread 0 issues
-// KD/16 MMAs (M = 128, N = 256, K = 16) into a 256-column TMEM accumulator and
-// commits to an mbarrier; each warp then reads its 32 rows back
-// (tcgen05.ld 32x32b) and keeps a running arg-min per row.  Every wait is
-// bounded; on timeout the CTA flags the error, frees its TMEM and returns.
+// One CTA (8 warps) owns 128 points: it converts them to BF16 into shared
+// memory in the core-matrix layout of tc_common.cuh while the first two tiles
+// of TN representatives (pre-converted once, contiguous) arrive by bulk
+// asynchronous copy; thread 0 issues KD/16 MMAs (M = 128, N = TN, K = 16)
+// per tile into one of two TMEM accumulators and commits to an mbarrier; the
+// warps read the rows back (tcgen05.ld 32x32b) and keep a running arg-min per
+// row while the next tile's MMA runs.  Every wait is bounded; on timeout the
+// CTA flags the error, frees its TMEM and returns.
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -63,24 +64,59 @@ __global__ void reps_to_bf16_tiles_kernel(const float4 *__restrict__ reps, int R
   rnorm[r] = r < R ? nrm : __int_as_float(0x7f800000);
 }
 
-__global__ void __launch_bounds__(128)
-    assign_tc_kernel(const float4 *__restrict__ rows, int64_t n, int dp4, int d, int KD,
+// Pipelined arg-min: 256 threads (8 warps) own 128 points.  The
+// representative tiles (pre-converted, contiguous) stream through two
+// shared-memory buffers by 1-D bulk asynchronous copies that complete on an
+// mbarrier transaction count; two TMEM accumulators of TN columns let the MMA
+// of tile j+1 run while the epilogue reads tile j.  Warps w and w+4 read the
+// same 32 TMEM lanes (rows) and split the TN columns; each thread keeps four
+// independent running minima (column c goes to chain c % 4), merged by
+// (value, index) at the end so ties still go to the lowest index.
+// dynamic shared memory: A tile, 2 B tiles, 2 x TN norms, 4 mbarriers,
+// TMEM slot, 128 (value, index) pairs
+__global__ void __launch_bounds__(256, 1)
+    assign_tc_kernel(const float4 *__restrict__ rows, int64_t n, int dp4, int d, int KD, int TN,
                      const __nv_bfloat16 *__restrict__ rep_tiles,
-                     const float *__restrict__ rnorm, int ntiles_r,
+                     const float *__restrict__ rnorm, int ntiles,
                      int32_t *__restrict__ cl, int *__restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  unsigned char *sa = smem;                                   // kTileM x KD
-  unsigned char *sb = sa + tc::tile_bytes(kTileM, KD);        // kTileN x KD
-  float *srn = reinterpret_cast<float *>(sb + tc::tile_bytes(kTileN, KD));
-  uint64_t *mbar = reinterpret_cast<uint64_t *>(srn + kTileN);
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 1);
+  const size_t a_bytes = tc::tile_bytes(kTileM, KD), b_bytes = tc::tile_bytes(TN, KD);
+  unsigned char *sa = smem;
+  unsigned char *sb0 = sa + a_bytes, *sb1 = sb0 + b_bytes;
+  float *sn0 = reinterpret_cast<float *>(sb1 + b_bytes), *sn1 = sn0 + TN;
+  auto sb = [&](int b) { return b ? sb1 : sb0; };
+  auto sn = [&](int b) { return b ? sn1 : sn0; };
+  uint64_t *full = reinterpret_cast<uint64_t *>(sn1 + TN);  // 2: copies landed
+  uint64_t *done = full + 2;                                    // 2: MMA finished
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 2);
+  float *pv = reinterpret_cast<float *>(tmem_slot + 4);         // 128 partial minima
+  int *pi = reinterpret_cast<int *>(pv + kTileM);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int quad = warp & 3, half = warp >> 2;
   const int64_t row0 = (int64_t)blockIdx.x * kTileM;
+  const uint32_t ncols = 2u * (uint32_t)TN;  // 256 or 512, a power of two
+  const uint32_t tile_tx = (uint32_t)(b_bytes + (size_t)TN * sizeof(float));
 
-  if (warp == 0) tc::tmem_alloc(tmem_slot, kTileN);
-  if (tid == 0) tc::mbar_init(mbar, 1);
-  // points -> BF16 core-matrix tile (thread = one row at a time, 8 columns)
+  if (warp == 0) tc::tmem_alloc(tmem_slot, ncols);
+  if (tid == 0) {
+    for (int i = 0; i < 2; i++) {
+      tc::mbar_init(full + i, 1);
+      tc::mbar_init(done + i, 1);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  // first two representative tiles in flight while the points are staged
+  if (tid == 0) {
+    for (int j = 0; j < 2 && j < ntiles; j++) {
+      tc::mbar_arrive_expect_tx(full + j, tile_tx);
+      tc::bulk_copy_g2s(sb(j), reinterpret_cast<const unsigned char *>(rep_tiles) + (size_t)j * b_bytes,
+                        (uint32_t)b_bytes, full + j);
+      tc::bulk_copy_g2s(sn(j), rnorm + (size_t)j * TN, (uint32_t)(TN * sizeof(float)), full + j);
+    }
+  }
+  // points -> BF16 core-matrix tile
   for (int t = tid; t < kTileM * (KD / 8); t += blockDim.x) {
     const int r = t / (KD / 8), k0 = (t % (KD / 8)) * 8;
     const int64_t gr = row0 + r;
@@ -98,67 +134,109 @@ __global__ void __launch_bounds__(128)
     *reinterpret_cast<uint4 *>(sa + tc::tile_offset(r, k0, KD)) =
         *reinterpret_cast<const uint4 *>(v);
   }
+  tc::fence_proxy_async_smem();
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = *tmem_slot;
-
-  const uint32_t idesc = tc::make_idesc_bf16(kTileM, kTileN);
-  const uint32_t a_base = tc::smem_u32(sa), b_base = tc::smem_u32(sb);
-  const uint32_t sbo = (uint32_t)KD * 16;  // next 8-row group
-  float best = __int_as_float(0x7f800000);
-  int best_j = 0;
+  const uint32_t idesc = tc::make_idesc_bf16(kTileM, TN);
+  const uint32_t a_base = tc::smem_u32(sa);
+  const uint32_t sbo = (uint32_t)KD * 16;
   bool ok = true;
-  const size_t btile = tc::tile_bytes(kTileN, KD);
-
-  for (int rt = 0; rt < ntiles_r && ok; rt++) {
-    // representative tile -> shared memory (contiguous copy) + its norms
-    const uint4 *src = reinterpret_cast<const uint4 *>(
-        reinterpret_cast<const unsigned char *>(rep_tiles) + (size_t)rt * btile);
-    uint4 *dst = reinterpret_cast<uint4 *>(sb);
-    for (int i = tid; i < (int)(btile / 16); i += blockDim.x) dst[i] = src[i];
-    for (int i = tid; i < kTileN; i += blockDim.x) srn[i] = rnorm[(size_t)rt * kTileN + i];
-    tc::fence_proxy_async_smem();
-    tc::fence_before_sync();
-    __syncthreads();
+  // MMA of tile j into accumulator j & 1 (thread 0), after its copy landed
+  auto issue = [&](int j) -> bool {
+    const int b = j & 1;
+    if (!tc::mbar_wait(full + b, (uint32_t)((j >> 1) & 1))) return false;
     tc::fence_after_sync();
-    if (tid == 0) {
-      for (int s = 0; s < KD / 16; s++) {
-        const uint64_t ad = tc::make_desc(a_base + 256u * s, 128u, sbo);
-        const uint64_t bd = tc::make_desc(b_base + 256u * s, 128u, sbo);
-        tc::mma_bf16(tmem, ad, bd, idesc, s > 0);
-      }
-      tc::mma_commit(mbar);
+    const uint32_t b_base = tc::smem_u32(sb(b));
+    for (int st = 0; st < KD / 16; st++) {
+      const uint64_t ad = tc::make_desc(a_base + 256u * st, 128u, sbo);
+      const uint64_t bd = tc::make_desc(b_base + 256u * st, 128u, sbo);
+      tc::mma_bf16(tmem + (uint32_t)(b * TN), ad, bd, idesc, st > 0);
     }
-    ok = tc::mbar_wait(mbar, (uint32_t)(rt & 1));
-    ok = __syncthreads_and(ok) != 0;  // one decision for the whole CTA
+    tc::mma_commit(done + b);
+    return true;
+  };
+  bool issued = true;
+  if (tid == 0 && ntiles > 0) issued = issue(0);
+  float best[4];
+  int bidx[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    best[c] = __int_as_float(0x7f800000);
+    bidx[c] = 0;
+  }
+  const int cbeg = half * (TN / 2);
+  for (int j = 0; j < ntiles; j++) {
+    const int b = j & 1;
+    if (tid == 0 && issued && j + 1 < ntiles) issued = issue(j + 1);
+    bool w = tc::mbar_wait(done + b, (uint32_t)((j >> 1) & 1));
+    ok = __syncthreads_and(w && (tid != 0 || issued)) != 0;
     if (!ok) break;
     tc::fence_after_sync();
-    // this warp's 32 rows, 32 columns at a time
-    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * TN + cbeg);
+    const float *nrm = sn(b) + cbeg;
+    const int jbase = j * TN + cbeg;
 #pragma unroll 1
-    for (int c = 0; c < kTileN; c += 32) {
+    for (int c0 = 0; c0 < TN / 2; c0 += 32) {
       float acc[32];
-      tc::tmem_ld_32x32(lane_base + (uint32_t)c, acc);
+      tc::tmem_ld_32x32(lane_base + (uint32_t)c0, acc);
 #pragma unroll
-      for (int j = 0; j < 32; j++) {
-        const float v = __fmaf_rn(-2.0f, acc[j], srn[c + j]);
-        if (v < best) {
-          best = v;
-          best_j = rt * kTileN + c + j;
+      for (int jj = 0; jj < 32; jj++) {
+        const float v = __fmaf_rn(-2.0f, acc[jj], nrm[c0 + jj]);
+        if (v < best[jj & 3]) {
+          best[jj & 3] = v;
+          bidx[jj & 3] = jbase + c0 + jj;
         }
       }
     }
     tc::fence_before_sync();
-    __syncthreads();  // TMEM and the B tile are reused by the next step
-    tc::fence_after_sync();
+    __syncthreads();  // accumulator b, tile b and its norms are free again
+    if (tid == 0 && j + 2 < ntiles) {
+      tc::fence_proxy_async_smem();
+      tc::mbar_arrive_expect_tx(full + b, tile_tx);
+      tc::bulk_copy_g2s(sb(b), reinterpret_cast<const unsigned char *>(rep_tiles) +
+                                   (size_t)(j + 2) * b_bytes,
+                        (uint32_t)b_bytes, full + b);
+      tc::bulk_copy_g2s(sn(b), rnorm + (size_t)(j + 2) * TN, (uint32_t)(TN * sizeof(float)),
+                        full + b);
+    }
   }
-  if (!ok && lane == 0) atomicExch(err, 1);
-  const int64_t gr = row0 + warp * 32 + lane;
-  if (gr < n) cl[gr] = ok ? best_j : 0;  // always a valid representative
+  // merge the chains: smallest value, then lowest index
+  float bv = best[0];
+  int bi = bidx[0];
+#pragma unroll
+  for (int c = 1; c < 4; c++)
+    if (best[c] < bv || (best[c] == bv && bidx[c] < bi)) {
+      bv = best[c];
+      bi = bidx[c];
+    }
+  const int rrow = quad * 32 + lane;
+  if (half == 1) {
+    pv[rrow] = bv;
+    pi[rrow] = bi;
+  }
+  __syncthreads();
+  if (half == 0) {
+    const float ov = pv[rrow];
+    const int oi = pi[rrow];
+    if (ov < bv || (ov == bv && oi < bi)) {
+      bv = ov;
+      bi = oi;
+    }
+    const int64_t gr = row0 + rrow;
+    // a point whose distances are all NaN keeps index 0: a valid cluster
+    if (gr < n) cl[gr] = ok ? bi : 0;
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+    // let the copies already issued land before the CTA's memory goes away
+    if (tid == 0)
+      for (int bb = 0; bb < 2; bb++) tc::mbar_wait(full + bb, 0), tc::mbar_wait(full + bb, 1);
+  }
   tc::fence_before_sync();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, kTileN);
+  if (warp == 0) tc::tmem_dealloc(tmem, ncols);
 }
 
 // Exact FP32 distance of every point to its chosen representative.
@@ -189,19 +267,23 @@ int launch_assign_tc(const float4 *rows, int64_t n, int dp4, int d, const float4
   reps_to_bf16_tiles_kernel<<<(Rpad + 127) / 128, 128, 0, s>>>(reps, R, dp4, d, KD, Rpad, tiles,
                                                                rnorm);
   KNN_LAUNCH_CHECK();
-  // at least 100 KB, so that no more than two CTAs (2 x 256 TMEM columns of
-  // the 512) share an SM and tcgen05.alloc never waits
-  const size_t need = tc::tile_bytes(kTileM, KD) + tc::tile_bytes(kTileN, KD) +
-                      kTileN * sizeof(float) + 16;
-  const size_t smem = std::max<size_t>(need, 100 * 1024);
+  // representative tiles of TN rows: two of them, the point tile and their
+  // norms must fit in shared memory (TN = 256 up to KD = 128)
+  const int TN = KD <= 128 ? kTileN : kTileN / 2;
+  const size_t need = tc::tile_bytes(kTileM, KD) + 2 * tc::tile_bytes(TN, KD) +
+                      2 * (size_t)TN * sizeof(float) + 4 * sizeof(uint64_t) + 16 +
+                      (size_t)kTileM * 8;
+  // a CTA holds 2 x TN TMEM columns: with TN = 256 that is all 512, so at
+  // most one CTA per SM (over 114 KB each), with TN = 128 at most two
+  const size_t smem = std::max<size_t>(need, TN == kTileN ? 116 * 1024 : 80 * 1024);
   KNN_CUDA_TRY(cudaFuncSetAttribute(assign_tc_kernel,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   KNN_CUDA_TRY(cudaFuncSetAttribute(assign_tc_kernel,
                                     cudaFuncAttributePreferredSharedMemoryCarveout,
                                     cudaSharedmemCarveoutMaxShared));
   const int64_t blocks = (n + kTileM - 1) / kTileM;
-  assign_tc_kernel<<<(unsigned)blocks, 128, smem, s>>>(rows, n, dp4, d, KD, tiles, rnorm,
-                                                       Rpad / kTileN, cl, err);
+  assign_tc_kernel<<<(unsigned)blocks, 256, smem, s>>>(rows, n, dp4, d, KD, TN, tiles, rnorm,
+                                                       Rpad / TN, cl, err);
   KNN_LAUNCH_CHECK();
   exact_rep_dist_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 32), 256, 0, s>>>(
       rows, n, dp4, reps, cl, dr);

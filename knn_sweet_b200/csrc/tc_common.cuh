@@ -98,6 +98,24 @@ __device__ __forceinline__ void mbar_init(uint64_t *mbar, uint32_t count) {
                : "memory");
 }
 
+// One arrival on the mbarrier that also expects `bytes` of asynchronous
+// copies to complete in the current phase.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+               :: "r"(smem_u32(mbar)), "r"(bytes) : "memory");
+}
+
+// 1-D bulk asynchronous copy global -> this CTA's shared memory (no
+// multicast), completing `bytes` of transaction count on the mbarrier.  Both
+// addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(void *dst_smem, const void *src_gmem,
+                                              uint32_t bytes, uint64_t *mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      :: "r"(smem_u32(dst_smem)), "l"(src_gmem), "r"(bytes), "r"(smem_u32(mbar))
+      : "memory");
+}
+
 // Bounded wait for the mbarrier phase with the given parity.  Returns false
 // when the wait gives up (about a second of spinning).
 __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
