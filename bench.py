@@ -59,6 +59,23 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(pg, value: float, device) -> float:
+    """Max of a per-rank float over all ranks (NCCL between GPUs, gloo on CPU);
+    every rank calls it at the same point."""
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def weak_scaling_value(world: int, points_per_rank: int, ms_per_step: float) -> float:
+    """Whole-job queries/s: every rank joins its own set of points_per_rank
+    queries; the step time is the slowest rank's."""
+    return world * points_per_rank / (ms_per_step * 1e-3)
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -258,13 +275,9 @@ def run_ours(args):
     if pg:
         pg.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = sum(step_ms)
-    if pg:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(pg, sum(step_ms), dev)
     ms_per_step = total_ms / args.steps
-    value = world * m / (ms_per_step * 1e-3)
+    value = weak_scaling_value(world, m, ms_per_step)
 
     # same steps with the library's own stage events (build / scan split),
     # giving the scan kernel's duration for the roofline
@@ -294,12 +307,8 @@ def run_ours(args):
             t0 = time.perf_counter()
             ks.knnjoin(qh, None, K, qreps=REPS, sreps=REPS, out=(oi, od))
             wall.append(time.perf_counter() - t0)
-        e2e_s = statistics.mean(wall)
-        if pg:
-            t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e = {"value": world * m / e2e_s, "unit": "queries/s",
+        e2e_s = max_over_ranks(pg, statistics.mean(wall), dev)
+        e2e = {"value": weak_scaling_value(world, m, e2e_s * 1e3), "unit": "queries/s",
                "h2d_bytes_per_step": int(x.nbytes), "d2h_bytes_per_step": int(m * K * 8),
                "ms_per_step": e2e_s * 1e3}
 

@@ -73,3 +73,63 @@ def knn_chamfer(x: torch.Tensor, y: torch.Tensor, k: int = 1) -> torch.Tensor:
     dxy, _ = knn_dist2(x, y, k)
     dyx, _ = knn_dist2(y, x, k)
     return dxy.sum() + dyx.sum()
+
+
+def _cloud_base(offsets, rows_off, device):
+    """Per query row: the first row of its cloud's reference points."""
+    import numpy as np
+    qo = np.asarray(rows_off, dtype=np.int64)
+    ro = np.asarray(offsets, dtype=np.int64)
+    counts = torch.from_numpy(np.diff(qo))
+    return torch.repeat_interleave(torch.from_numpy(ro[:-1]), counts).to(device)
+
+
+class _KnnDist2Batched(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, queries, q_offsets, sources, r_offsets, k):
+        from .batched import knnjoin_batched
+        q = queries.detach().contiguous()
+        s = sources.detach().contiguous()
+        idx, d2 = knnjoin_batched(q, q_offsets, s, r_offsets, k, squared=True)
+        # indices relative to each cloud -> rows of the concatenated sources
+        base = _cloud_base(r_offsets, q_offsets, q.device).to(torch.int32)
+        gidx = torch.where(idx >= 0, idx + base[:, None], idx)
+        ctx.save_for_backward(q, s, gidx)
+        ctx.mark_non_differentiable(idx)
+        return d2, idx
+
+    @staticmethod
+    def backward(ctx, grad_d2, _grad_idx):
+        q, s, gidx = ctx.saved_tensors
+        m, d = q.shape
+        n, k = s.shape[0], gidx.shape[1]
+        g = torch.where(gidx >= 0, grad_d2.contiguous().to(torch.float32),
+                        torch.zeros_like(grad_d2, dtype=torch.float32))
+        grad_q = torch.zeros_like(q)
+        grad_s = torch.zeros_like(s) if ctx.needs_input_grad[2] else None
+        lib = _lib.load()
+        with torch.cuda.device(q.device):
+            stream = ctypes.c_void_p(torch.cuda.current_stream(q.device).cuda_stream)
+            rc = lib.knn_backward_device(_ptr(q), m, _ptr(s), n, d, k, _ptr(gidx), _ptr(g),
+                                         _ptr(grad_q),
+                                         _ptr(grad_s) if grad_s is not None else None, stream)
+        _lib.check(rc)
+        return grad_q, None, grad_s, None, None
+
+
+def knn_dist2_batched(queries, q_offsets, sources, r_offsets, k: int):
+    """Batched (d2, idx) over many cloud pairs: cloud c's queries
+    q_offsets[c]:q_offsets[c+1] against its sources r_offsets[c]:r_offsets[c+1];
+    idx relative to the cloud's first source row; d2 differentiable in both point
+    sets (one forward call for all clouds, one backward launch)."""
+    if not (queries.is_cuda and sources.is_cuda):
+        raise ValueError("knn_dist2_batched needs CUDA tensors")
+    return _KnnDist2Batched.apply(queries, q_offsets, sources, r_offsets, k)
+
+
+def knn_chamfer_batched(x, x_offsets, y, y_offsets, k: int = 1) -> torch.Tensor:
+    """Per-pair Chamfer-type losses of many cloud pairs, summed: for every pair c,
+    the k nearest squared distances from x_c to y_c and from y_c to x_c."""
+    dxy, _ = knn_dist2_batched(x, x_offsets, y, y_offsets, k)
+    dyx, _ = knn_dist2_batched(y, y_offsets, x, x_offsets, k)
+    return dxy.sum() + dyx.sum()

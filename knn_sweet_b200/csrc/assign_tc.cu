@@ -12,7 +12,7 @@
 //
 // One CTA (8 warps) owns 128 points: it converts them to BF16 into shared
 // memory in the core-matrix layout of tc_common.cuh while the first two tiles
-// of TN representatives (pre-converted once, contiguous) arrive by bulk
+// of TN = 128 representatives (pre-converted once, contiguous) arrive by bulk
 // asynchronous copy; thread 0 issues KD/16 MMAs (M = 128, N = TN, K = 16)
 // per tile into one of two TMEM accumulators and commits to an mbarrier; the
 // warps read the rows back (tcgen05.ld 32x32b) and keep a running arg-min per
@@ -267,9 +267,10 @@ int launch_assign_tc(const float4 *rows, int64_t n, int dp4, int d, const float4
   reps_to_bf16_tiles_kernel<<<(Rpad + 127) / 128, 128, 0, s>>>(reps, R, dp4, d, KD, Rpad, tiles,
                                                                rnorm);
   KNN_LAUNCH_CHECK();
-  // representative tiles of TN rows: two of them, the point tile and their
-  // norms must fit in shared memory (TN = 256 up to KD = 128)
-  const int TN = KD <= 128 ? kTileN : kTileN / 2;
+  // representative tiles of 128 rows: a CTA then holds 256 TMEM columns and
+  // two CTAs share an SM, whose warps hide each other's epilogue latency
+  // (measured faster than 256-row tiles with one CTA per SM)
+  const int TN = kTileN / 2;
   const size_t need = tc::tile_bytes(kTileM, KD) + 2 * tc::tile_bytes(TN, KD) +
                       2 * (size_t)TN * sizeof(float) + 4 * sizeof(uint64_t) + 16 +
                       (size_t)kTileM * 8;
