@@ -216,6 +216,30 @@ int knn_join_batched_device(const float *q, const int64_t *q_offsets,
                             void *stream);
 
 /*
+ * Reusable index of a reference set.  The reference rebuilds everything on
+ * every run (clusterReps, src/knnjoin.cu:166-411), although its source side --
+ * representatives, assignment, sorted member lists (knnjoin.cu:223-240,
+ * 331-399) -- depends only on the reference points.  knn_index_build does that
+ * part once, on the current device and `stream`, keeping a copy of the points;
+ * it returns when the build is complete.  Options that shape it: sreps, seed,
+ * rep_trials, lloyd_iters, KNN_NO_TENSOR_CORES.
+ * knn_index_query then joins any number of query batches against it: the same
+ * result as knn_join_device with the same options (the query-side options:
+ * qreps, precision, margin, KNN_SQUARED_DIST), device buffers, enqueued on
+ * `stream`; it must run on the index's device.  Queries may run concurrently
+ * on different streams (the index is read-only).  knn_index_free releases the
+ * index (it synchronises); knn_index_info reports n, d and the representatives.
+ */
+typedef struct knn_index knn_index;
+int knn_index_build(const float *r, int64_t n, int32_t d, const knn_options *opt,
+                    knn_index **out, void *stream);
+int knn_index_query(const knn_index *index, const float *q, int64_t m, int32_t k,
+                    int32_t *out_idx, float *out_dist, const knn_options *opt,
+                    knn_stats *st, void *stream);
+int knn_index_free(knn_index *index);
+int knn_index_info(const knn_index *index, int64_t *n, int32_t *d, int32_t *reps);
+
+/*
  * Returns the device scratch memory the library keeps cached between calls
  * (one stream-ordered pool per device; no reference counterpart: the
  * reference never frees its device memory).  Memory still in use by calls in

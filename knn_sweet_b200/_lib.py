@@ -80,6 +80,13 @@ SIGNATURES = {
     "knn_trim_memory": (_c_int, []),
     "knn_join_device_noalloc": (_c_int, [_vp, _c_i64, _vp, _c_i64, _c_i32, _c_i32, _vp, _vp,
                                          ctypes.POINTER(KnnOptions), _vp]),
+    "knn_index_build": (_c_int, [_vp, _c_i64, _c_i32, ctypes.POINTER(KnnOptions),
+                                 ctypes.POINTER(_vp), _vp]),
+    "knn_index_query": (_c_int, [_vp, _vp, _c_i64, _c_i32, _vp, _vp,
+                                 ctypes.POINTER(KnnOptions), ctypes.POINTER(KnnStats), _vp]),
+    "knn_index_free": (_c_int, [_vp]),
+    "knn_index_info": (_c_int, [_vp, ctypes.POINTER(_c_i64), ctypes.POINTER(_c_i32),
+                                ctypes.POINTER(_c_i32)]),
     "knn_join_batched_device": (_c_int, [_vp, _vp, _vp, _vp, _c_i32, _c_i32, _c_i32, _vp, _vp,
                                          ctypes.POINTER(KnnOptions),
                                          ctypes.POINTER(KnnStats), _vp]),

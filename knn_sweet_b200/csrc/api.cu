@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <vector>
 
 #include "common.cuh"
@@ -89,6 +90,13 @@ class Arena {
   }
   Arena(const Arena &) = delete;
   Arena &operator=(const Arena &) = delete;
+
+  // Hands the allocations made so far to the caller: they outlive the arena.
+  std::vector<void *> take() {
+    std::vector<void *> out;
+    out.swap(ptrs_);
+    return out;
+  }
 
   template <class T>
   int alloc(T **out, size_t count) {
@@ -174,7 +182,7 @@ struct ClusterSet {
   int32_t *off = nullptr;     // R + 1
 };
 
-int build_clusters(Arena &ar, const float4 *rows, int64_t n, int d, int dp4s, int R,
+int build_clusters(Arena &keep, Arena &ar, const float4 *rows, int64_t n, int d, int dp4s, int R,
                    uint32_t seed, int trials, int lloyd_iters, bool use_tc, int *err,
                    cudaStream_t s, ClusterSet *cs) {
   cs->R = R;
@@ -187,8 +195,8 @@ int build_clusters(Arena &ar, const float4 *rows, int64_t n, int d, int dp4s, in
   KNN_TRY(ar.alloc(&cand_dev, cand.size()));
   KNN_TRY(ar.alloc(&score, (size_t)trials));
   KNN_TRY(upload_i32(cand, cand_dev, s));
-  KNN_TRY(ar.alloc(&cs->reps, (size_t)R * dp4s));
-  KNN_TRY(ar.alloc(&cs->rep_rows, (size_t)R));
+  KNN_TRY(keep.alloc(&cs->reps, (size_t)R * dp4s));
+  KNN_TRY(keep.alloc(&cs->rep_rows, (size_t)R));
   KNN_TRY(launch_rep_select(rows, dp4s, cand_dev, R, trials, score, cs->reps,
                             cs->rep_rows, s));
   int32_t *cl;
@@ -202,12 +210,12 @@ int build_clusters(Arena &ar, const float4 *rows, int64_t n, int d, int dp4s, in
   int32_t *vals;
   KNN_TRY(ar.alloc(&keys, (size_t)n));
   KNN_TRY(ar.alloc(&vals, (size_t)n));
-  KNN_TRY(ar.alloc(&cs->skeys, (size_t)n));
-  KNN_TRY(ar.alloc(&cs->perm, (size_t)n));
+  KNN_TRY(keep.alloc(&cs->skeys, (size_t)n));
+  KNN_TRY(keep.alloc(&cs->perm, (size_t)n));
   size_t temp_bytes = cluster_sort_temp_bytes(n, R);
   unsigned char *temp;
   KNN_TRY(ar.alloc(&temp, temp_bytes));
-  KNN_TRY(ar.alloc(&cs->off, (size_t)R + 1));
+  KNN_TRY(keep.alloc(&cs->off, (size_t)R + 1));
   // nearest representative (BF16 tensor-core arg-min + exact FP32 distance to
   // the winner for d >= 16, FP32 CUDA cores otherwise), then one sort into
   // clusters; with Lloyd steps the representatives move to their clusters'
@@ -318,6 +326,86 @@ struct ChunkEvents {
   }
 };
 
+// Row geometry: float4 chunks per row (rounded up to a power of two for the
+// register-width scan kernels when d <= 32) and the scan template width.
+void row_geometry(int d, int *dp4s, int *tmpl) {
+  const int dp4 = (d + 3) / 4;
+  *dp4s = dp4;
+  *tmpl = 0;
+  if (dp4 <= 8) {
+    int p = 1;
+    while (p < dp4) p <<= 1;
+    *dp4s = p;
+    *tmpl = p;
+  }
+}
+
+// The reference side of a join: representatives, clusters, the
+// cluster-contiguous rows and their bounds.  Depends only on the reference
+// set and the options that shape its clusters.
+struct RefSide {
+  int64_t n = 0;
+  int d = 0, dp4s = 0, tmpl = 0, Rs = 0;
+  bool idx_in_row = false;
+  ClusterSet sset;
+  const float4 *Rp = nullptr;  // packed rows, original order
+  float4 *srows = nullptr;     // cluster-contiguous rows
+  float *sdist = nullptr, *cmin = nullptr, *cmax = nullptr;
+  int32_t *sidx = nullptr;
+};
+
+// Builds the reference side; the arrays it keeps come from `keep`, scratch
+// from `tmp`.  With copy_rows the packed rows are always a copy (an index
+// must not depend on the caller's buffer).
+int build_ref_side(Arena &keep, Arena &tmp, const float *r, int64_t n, int d, int Rs,
+                   const knn_options &o, bool copy_rows, int *dev_err, cudaStream_t s,
+                   RefSide *R) {
+  R->n = n;
+  R->d = d;
+  row_geometry(d, &R->dp4s, &R->tmpl);
+  R->Rs = Rs;
+  const int dp4s = R->dp4s;
+  if (!copy_rows && dp4s * 4 == d && (reinterpret_cast<uintptr_t>(r) & 15) == 0) {
+    R->Rp = reinterpret_cast<const float4 *>(r);
+  } else {
+    float4 *p;
+    KNN_TRY(keep.alloc(&p, (size_t)n * dp4s));
+    KNN_TRY(launch_pack_rows(r, n, d, dp4s, p, s));
+    R->Rp = p;
+  }
+  const bool use_tc = (o.flags & KNN_NO_TENSOR_CORES) == 0;
+  KNN_TRY(build_clusters(keep, tmp, R->Rp, n, d, dp4s, Rs, o.seed, o.rep_trials, o.lloyd_iters,
+                         use_tc, dev_err, s, &R->sset));
+  KNN_TRY(keep.alloc(&R->srows, (size_t)n * dp4s));
+  KNN_TRY(keep.alloc(&R->sdist, (size_t)n));
+  KNN_TRY(keep.alloc(&R->sidx, (size_t)n));
+  KNN_TRY(keep.alloc(&R->cmin, (size_t)Rs));
+  KNN_TRY(keep.alloc(&R->cmax, (size_t)Rs));
+  // rows with a spare pad float carry their index there (register-width rows)
+  R->idx_in_row = R->tmpl > 0 && 4 * dp4s > d;
+  KNN_TRY(launch_cluster_layout(R->sset.skeys, R->sset.perm, n, R->Rp, dp4s, R->idx_in_row,
+                                R->srows, R->sdist, R->sidx, s));
+  KNN_TRY(launch_cluster_minmax(R->sset.off, R->sdist, Rs, R->cmin, R->cmax, s));
+  return KNN_OK;
+}
+
+// Number of query representatives for m queries (self: the join shares the
+// reference clusters when the counts agree).
+int query_rep_count(const knn_options &o, int64_t m, int d, int k, bool self, int Rs) {
+  int Rq = o.qreps > 0 ? o.qreps : (self ? Rs : default_reps(m));
+  // the tensor-core tiles hold 128 queries of one query cluster: by default
+  // the BF16 form sizes the query clusters to fill them
+  if (o.qreps <= 0 && !self && o.precision == KNN_BF16_REFINE && tile_search_supported(d, k, o.margin))
+    Rq = (int)std::min<int64_t>(KNN_MAX_REPS, std::max<int64_t>(1, (m + 127) / 128));
+  if (Rq > m) Rq = (int)m;
+  return Rq;
+}
+
+int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t k,
+               int32_t *out_idx, float *out_dist, const knn_options &o, knn_stats *st,
+               cudaStream_t s, HostSink *sink, Arena &ar, EventSet &evs,
+               unsigned long long *ctr);
+
 int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
                      int32_t d, int32_t k, int32_t *out_idx, float *out_dist,
                      const knn_options *opt, knn_stats *st, cudaStream_t s,
@@ -338,79 +426,64 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
     KNN_LAUNCH_CHECK();
     return KNN_OK;
   }
-  int dev = 0, num_sms = 148;
-  KNN_CUDA_TRY(cudaGetDevice(&dev));
-  KNN_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
-
-  const int dp4 = (d + 3) / 4;
-  int dp4s = dp4, tmpl = 0;
-  if (dp4 <= 8) {
-    dp4s = 1;
-    while (dp4s < dp4) dp4s <<= 1;
-    tmpl = dp4s;
-  }
   const bool self = (q == r) && (m == n);
   int Rs = o.sreps > 0 ? o.sreps : default_reps(n);
-  int Rq = o.qreps > 0 ? o.qreps : (self ? Rs : default_reps(m));
-  // the tensor-core tiles hold 128 queries of one query cluster: by default
-  // the BF16 form sizes the query clusters to fill them
-  if (o.qreps <= 0 && !self && o.precision == KNN_BF16_REFINE && tile_search_supported(d, k, o.margin))
-    Rq = (int)std::min<int64_t>(KNN_MAX_REPS, std::max<int64_t>(1, (m + 127) / 128));
   if (Rs > n) Rs = (int)n;
-  if (Rq > m) Rq = (int)m;
+  const int Rq = query_rep_count(o, m, d, k, self, Rs);
   const bool share = self && Rq == Rs;
 
   EventSet evs;
   if (st) KNN_TRY(evs.create());
   KNN_TRY(evs.record(0, s));
   Arena ar(s);
-
-  // packed rows (aliased when the input rows already are float4 rows)
-  auto packed = [&](const float *src, int64_t cnt, const float4 **outp) -> int {
-    if (dp4s * 4 == d && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
-      *outp = reinterpret_cast<const float4 *>(src);
-      return KNN_OK;
-    }
-    float4 *p;
-    KNN_TRY(ar.alloc(&p, (size_t)cnt * dp4s));
-    KNN_TRY(launch_pack_rows(src, cnt, d, dp4s, p, s));
-    *outp = p;
-    return KNN_OK;
-  };
   // [0] work counter, [1..5] statistics, [6] device error flag, [7] tile
   // counter, [8..11] tile statistics, [12] count of slots left to the scan
   unsigned long long *ctr;
   KNN_TRY(ar.alloc(&ctr, 13));
   KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, 13 * sizeof(unsigned long long), s));
+  RefSide R;
+  KNN_TRY(build_ref_side(ar, ar, r, n, d, Rs, o, false, reinterpret_cast<int *>(ctr + 6), s, &R));
+  return query_impl(R, share, q, m, k, out_idx, out_dist, o, st, s, sink, ar, evs, ctr);
+}
+
+// The query side of a join against a built reference side.  `ctr` (13
+// counters, zeroed) and the events come from the caller; event 0 is recorded.
+int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t k,
+               int32_t *out_idx, float *out_dist, const knn_options &o, knn_stats *st,
+               cudaStream_t s, HostSink *sink, Arena &ar, EventSet &evs,
+               unsigned long long *ctr) {
+  const int64_t n = R.n;
+  const int d = R.d, dp4s = R.dp4s, tmpl = R.tmpl, Rs = R.Rs;
+  const bool idx_in_row = R.idx_in_row;
+  const ClusterSet &sset = R.sset;
+  const float4 *Rp = R.Rp;
+  float4 *srows = R.srows;
+  float *sdist = R.sdist, *cmin = R.cmin, *cmax = R.cmax;
+  int32_t *sidx = R.sidx;
+  if (st) st->pairs_total = m * n;
+  int dev = 0, num_sms = 148;
+  KNN_CUDA_TRY(cudaGetDevice(&dev));
+  KNN_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+  const bool self_rows = share;
+  const int Rq = share ? Rs : query_rep_count(o, m, d, k, false, Rs);
   int *dev_err = reinterpret_cast<int *>(ctr + 6);
   const bool use_tc = (o.flags & KNN_NO_TENSOR_CORES) == 0;
-
-  const float4 *Rp = nullptr, *Qp = nullptr;
-  KNN_TRY(packed(r, n, &Rp));
-  ClusterSet sset, qset;
-  KNN_TRY(build_clusters(ar, Rp, n, d, dp4s, Rs, o.seed, o.rep_trials, o.lloyd_iters, use_tc, dev_err, s,
-                         &sset));
-  float4 *srows;
-  float *sdist, *cmin, *cmax;
-  int32_t *sidx;
-  KNN_TRY(ar.alloc(&srows, (size_t)n * dp4s));
-  KNN_TRY(ar.alloc(&sdist, (size_t)n));
-  KNN_TRY(ar.alloc(&sidx, (size_t)n));
-  KNN_TRY(ar.alloc(&cmin, (size_t)Rs));
-  KNN_TRY(ar.alloc(&cmax, (size_t)Rs));
-  // rows with a spare pad float carry their index there (register-width rows)
-  const bool idx_in_row = tmpl > 0 && 4 * dp4s > d;
-  KNN_TRY(launch_cluster_layout(sset.skeys, sset.perm, n, Rp, dp4s, idx_in_row, srows,
-                                sdist, sidx, s));
-  KNN_TRY(launch_cluster_minmax(sset.off, sdist, Rs, cmin, cmax, s));
-
-  if (share) {
+  const float4 *Qp = nullptr;
+  ClusterSet qset;
+  if (self_rows) {
     Qp = Rp;
     qset = sset;
   } else {
-    KNN_TRY(packed(q, m, &Qp));
-    KNN_TRY(build_clusters(ar, Qp, m, d, dp4s, Rq, o.seed, o.rep_trials, o.lloyd_iters, use_tc, dev_err, s,
-                           &qset));
+    if (dp4s * 4 == d && (reinterpret_cast<uintptr_t>(q) & 15) == 0) {
+      Qp = reinterpret_cast<const float4 *>(q);
+    } else {
+      float4 *p;
+      KNN_TRY(ar.alloc(&p, (size_t)m * dp4s));
+      KNN_TRY(launch_pack_rows(q, m, d, dp4s, p, s));
+      Qp = p;
+    }
+    KNN_TRY(build_clusters(ar, ar, Qp, m, d, dp4s, Rq, o.seed, o.rep_trials, o.lloyd_iters,
+                           use_tc, dev_err, s, &qset));
   }
   float *qrad, *drr, *theta0;
   int32_t *slot_cl, *rlist, *rlen;
@@ -593,12 +666,149 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
   return KNN_OK;
 }
 
+// Index build / query (the reusable reference side).
+int index_build_impl(const float *r, int64_t n, int32_t d, const knn_options &o,
+                     cudaStream_t s, RefSide *R, std::vector<void *> *mem) {
+  int Rs = o.sreps > 0 ? o.sreps : default_reps(n);
+  if (Rs > n) Rs = (int)n;
+  Arena keep(s);
+  int rc = KNN_OK;
+  {
+    Arena tmp(s);
+    int *err = nullptr;
+    rc = tmp.alloc(&err, 1);
+    if (rc == KNN_OK && cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess) {
+      set_error("cudaMemsetAsync failed");
+      rc = KNN_ECUDA;
+    }
+    if (rc == KNN_OK) rc = build_ref_side(keep, tmp, r, n, d, Rs, o, true, err, s, R);
+    int h = 0;
+    if (rc == KNN_OK && (cudaMemcpyAsync(&h, err, sizeof h, cudaMemcpyDeviceToHost, s) !=
+                             cudaSuccess ||
+                         cudaStreamSynchronize(s) != cudaSuccess)) {
+      set_error("index build failed on the device: %s", cudaGetErrorString(cudaGetLastError()));
+      rc = KNN_ECUDA;
+    }
+    if (rc == KNN_OK && h != 0) {
+      set_error("a bounded device wait gave up (tensor-core pipeline)");
+      rc = KNN_ETIMEOUT;
+    }
+  }
+  if (rc == KNN_OK) *mem = keep.take();
+  return rc;
+}
+
 }  // namespace
 }  // namespace knnsweet
 
 using namespace knnsweet;
 
+// Opaque index: the reference side of the join, kept on one device.
+struct knn_index {
+  int device = 0;
+  RefSide *ref = nullptr;
+  std::vector<void *> mem;
+};
+
 extern "C" {
+
+int knn_index_build(const float *r, int64_t n, int32_t d, const knn_options *opt,
+                    knn_index **out, void *stream) {
+  error_buffer().clear();
+  launch_counter() = 0;
+  if (!out) {
+    set_error("null index pointer");
+    return KNN_EINVAL;
+  }
+  *out = nullptr;
+  knn_options o;
+  KNN_TRY(check_options(opt, &o));
+  KNN_TRY(check_sizes(1, n, d, 1));
+  if (n <= 0 || !r) {
+    set_error("an index needs n >= 1 reference points and a device pointer");
+    return KNN_EINVAL;
+  }
+  auto *idx = new (std::nothrow) knn_index;
+  auto *R = new (std::nothrow) RefSide;
+  if (!idx || !R) {
+    delete idx;
+    delete R;
+    set_error("host allocation failed");
+    return KNN_ENOMEM;
+  }
+  KNN_CUDA_TRY(cudaGetDevice(&idx->device));
+  const int rc = index_build_impl(r, n, d, o, static_cast<cudaStream_t>(stream), R, &idx->mem);
+  if (rc != KNN_OK) {
+    delete R;
+    delete idx;
+    return rc;
+  }
+  idx->ref = R;
+  *out = idx;
+  return KNN_OK;
+}
+
+int knn_index_query(const knn_index *index, const float *q, int64_t m, int32_t k,
+                    int32_t *out_idx, float *out_dist, const knn_options *opt, knn_stats *st,
+                    void *stream) {
+  error_buffer().clear();
+  if (st) memset(st, 0, sizeof *st);
+  launch_counter() = 0;
+  if (!index || !index->ref) {
+    set_error("null index");
+    return KNN_EINVAL;
+  }
+  knn_options o;
+  KNN_TRY(check_options(opt, &o));
+  KNN_TRY(check_sizes(m, index->ref->n, index->ref->d, k));
+  if (m == 0) return KNN_OK;
+  if (!q || !out_idx || !out_dist) {
+    set_error("null pointer argument");
+    return KNN_EINVAL;
+  }
+  int dev = 0;
+  KNN_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev != index->device) {
+    set_error("the index lives on device %d, the current device is %d", index->device, dev);
+    return KNN_EINVAL;
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  EventSet evs;
+  if (st) KNN_TRY(evs.create());
+  KNN_TRY(evs.record(0, s));
+  Arena ar(s);
+  unsigned long long *ctr;
+  KNN_TRY(ar.alloc(&ctr, 13));
+  KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, 13 * sizeof(unsigned long long), s));
+  return query_impl(*index->ref, false, q, m, k, out_idx, out_dist, o, st, s, nullptr, ar, evs,
+                    ctr);
+}
+
+int knn_index_free(knn_index *index) {
+  if (!index) return KNN_OK;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(index->device);
+  int rc = KNN_OK;
+  for (void *p : index->mem)
+    if (cudaFree(p) != cudaSuccess) rc = KNN_ECUDA;
+  cudaSetDevice(prev);
+  delete index->ref;
+  delete index;
+  if (rc != KNN_OK) set_error("cudaFree failed while releasing an index");
+  return rc;
+}
+
+int knn_index_info(const knn_index *index, int64_t *n, int32_t *d, int32_t *reps) {
+  if (!index || !index->ref) {
+    set_error("null index");
+    return KNN_EINVAL;
+  }
+  if (n) *n = index->ref->n;
+  if (d) *d = index->ref->d;
+  if (reps) *reps = index->ref->Rs;
+  return KNN_OK;
+}
 
 void knn_default_options(knn_options *opt) {
   if (!opt) return;

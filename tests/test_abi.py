@@ -152,3 +152,14 @@ def test_batched_bad_options_rejected():
         o = _lib.default_options()
         setattr(o, field, val)
         assert _call_batched([0, 10], [0, 10], 1, 3, 4, opt=o) == _lib.KNN_EINVAL, field
+
+
+def test_index_argument_errors_without_gpu():
+    lib = _lib.load()
+    assert lib.knn_index_free(None) == _lib.KNN_OK
+    h = ctypes.c_void_p()
+    assert lib.knn_index_build(None, 10, 3, None, ctypes.byref(h), None) == _lib.KNN_EINVAL
+    assert lib.knn_index_build(None, 10, 0, None, ctypes.byref(h), None) == _lib.KNN_EINVAL
+    assert lib.knn_index_build(None, 10, 3, None, None, None) == _lib.KNN_EINVAL
+    assert lib.knn_index_query(None, None, 5, 3, None, None, None, None, None) == _lib.KNN_EINVAL
+    assert lib.knn_index_info(None, None, None, None) == _lib.KNN_EINVAL

@@ -124,9 +124,12 @@ def test_batched_chamfer_matches_per_pair(cuda_device, k):
         b = b.clone().requires_grad_(True)
         l = knn_chamfer(a, b, k)
         l.backward()
-        ref_loss += float(l)
+        ref_loss += float(l.detach())
         gx.append(a.grad)
         gy.append(b.grad)
-    assert float(loss) == pytest.approx(ref_loss, rel=1e-5)
-    torch.testing.assert_close(x.grad, torch.cat(gx), rtol=1e-5, atol=1e-6)
-    torch.testing.assert_close(y.grad, torch.cat(gy), rtol=1e-5, atol=1e-6)
+    assert float(loss.detach()) == pytest.approx(ref_loss, rel=1e-5)
+    # gradients of reference points are sums over every query that picked them,
+    # accumulated with float atomics: the order of those additions differs
+    # between the two runs
+    torch.testing.assert_close(x.grad, torch.cat(gx), rtol=1e-4, atol=1e-5)
+    torch.testing.assert_close(y.grad, torch.cat(gy), rtol=1e-4, atol=1e-5)
