@@ -46,47 +46,50 @@ __global__ void pack_rows_kernel(const float *__restrict__ src, int64_t n,
 // Representative draw (src/knnjoin.cu:125-154, host draw 195-239).
 // cand[t * R + i] are row indices drawn on the host with the glibc generator.
 // score[t] = wrapping int32 sum over ordered pairs (i, j) of (int)dist.
-// Tiled: a block owns 64 x 64 candidate pairs of one trial; rows are staged
-// through shared memory 32 floats at a time and every thread accumulates 16
-// pairs (i = i0 + ty + 16a, j = j0 + tx + 16b), each summed in dimension
-// order with fma, exactly as the one-pair distance would be.
-// grid: (ceil(R / 64), ceil(R / 64), trials), 256 threads
+// Tiled: a block owns (16 TB) x (16 TB) candidate pairs of one trial; rows are
+// staged through shared memory 32 floats at a time and every thread
+// accumulates TB x TB pairs (i = i0 + ty + 16a, j = j0 + tx + 16b), each
+// summed in dimension order with fma, exactly as the one-pair distance would
+// be.
+// grid: (ceil(R / 16TB), ceil(R / 16TB), trials), 256 threads
 // ---------------------------------------------------------------------------
+template <int TB>
 __global__ void __launch_bounds__(256)
     rep_score_kernel(const float4 *__restrict__ rows, int dp4,
                      const int32_t *__restrict__ cand, int R,
                      uint32_t *__restrict__ score) {
-  __shared__ float4 sa[8][64];
-  __shared__ float4 sb[8][64];
+  constexpr int T = 16 * TB;
+  __shared__ float4 sa[8][T];
+  __shared__ float4 sb[8][T];
   __shared__ uint32_t red[8];
   const int t = blockIdx.z;
-  const int i0 = blockIdx.x * 64, j0 = blockIdx.y * 64;
+  const int i0 = blockIdx.x * T, j0 = blockIdx.y * T;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int32_t *c = cand + (int64_t)t * R;
-  float acc[4][4];
+  float acc[TB][TB];
 #pragma unroll
-  for (int a = 0; a < 4; a++)
+  for (int a = 0; a < TB; a++)
 #pragma unroll
-    for (int b = 0; b < 4; b++) acc[a][b] = 0.0f;
+    for (int b = 0; b < TB; b++) acc[a][b] = 0.0f;
   for (int ch = 0; ch < dp4; ch += 8) {
     const int nch = min(8, dp4 - ch);
-    for (int e = threadIdx.x; e < 64 * 8; e += 256) {
-      const int r = e & 63, q = e >> 6;
+    for (int e = threadIdx.x; e < T * 8; e += 256) {
+      const int r = e % T, q = e / T;
       const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
       sa[q][r] = (q < nch && i0 + r < R) ? rows[(int64_t)c[i0 + r] * dp4 + ch + q] : zero;
       sb[q][r] = (q < nch && j0 + r < R) ? rows[(int64_t)c[j0 + r] * dp4 + ch + q] : zero;
     }
     __syncthreads();
     for (int q = 0; q < nch; q++) {
-      float4 av[4], bv[4];
+      float4 av[TB], bv[TB];
 #pragma unroll
-      for (int a = 0; a < 4; a++) av[a] = sa[q][ty + 16 * a];
+      for (int a = 0; a < TB; a++) av[a] = sa[q][ty + 16 * a];
 #pragma unroll
-      for (int b = 0; b < 4; b++) bv[b] = sb[q][tx + 16 * b];
+      for (int b = 0; b < TB; b++) bv[b] = sb[q][tx + 16 * b];
 #pragma unroll
-      for (int a = 0; a < 4; a++)
+      for (int a = 0; a < TB; a++)
 #pragma unroll
-        for (int b = 0; b < 4; b++) {
+        for (int b = 0; b < TB; b++) {
           float s = acc[a][b], u;
           u = __fsub_rn(av[a].x, bv[b].x); s = __fmaf_rn(u, u, s);
           u = __fsub_rn(av[a].y, bv[b].y); s = __fmaf_rn(u, u, s);
@@ -99,9 +102,9 @@ __global__ void __launch_bounds__(256)
   }
   uint32_t sum = 0;
 #pragma unroll
-  for (int a = 0; a < 4; a++)
+  for (int a = 0; a < TB; a++)
 #pragma unroll
-    for (int b = 0; b < 4; b++)
+    for (int b = 0; b < TB; b++)
       if (i0 + ty + 16 * a < R && j0 + tx + 16 * b < R)
         sum += (uint32_t)(int32_t)sqrtf(acc[a][b]);
   // block reduce (wrapping unsigned add), one atomic per block
@@ -230,34 +233,41 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(256)
     centroid_kernel(const float4 *__restrict__ rows, int dp4, const int32_t *__restrict__ perm,
                     const int32_t *__restrict__ off, float4 *__restrict__ reps) {
+  // G = pow2 >= dp4 lanes read one member row (one float4 each, coalesced);
+  // 256 / G groups take every (256/G)-th member; the groups' partial sums are
+  // added in group order, so the result does not depend on scheduling.
   __shared__ float4 red[256];
   const int c = blockIdx.x, tid = threadIdx.x;
   const int a = off[c], b = off[c + 1];
   if (b == a) return;
-  const float inv = 1.0f / (float)(b - a);
-  for (int ch = 0; ch < dp4; ch++) {
+  int G = 1;
+  while (G < dp4 && G < 256) G <<= 1;
+  const int groups = 256 / G, g = tid / G, col = tid % G;
+  for (int c0 = 0; c0 < dp4; c0 += G) {
+    const int ch = c0 + col;
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int p = a + tid; p < b; p += 256) {
-      const float4 v = rows[(int64_t)perm[p] * dp4 + ch];
-      acc.x += v.x;
-      acc.y += v.y;
-      acc.z += v.z;
-      acc.w += v.w;
-    }
+    if (ch < dp4 && g < groups)
+      for (int p = a + g; p < b; p += groups) {
+        const float4 v = rows[(int64_t)perm[p] * dp4 + ch];
+        acc.x += v.x;
+        acc.y += v.y;
+        acc.z += v.z;
+        acc.w += v.w;
+      }
     red[tid] = acc;
     __syncthreads();
-    for (int s = 128; s > 0; s >>= 1) {
-      if (tid < s) {
-        red[tid].x += red[tid + s].x;
-        red[tid].y += red[tid + s].y;
-        red[tid].z += red[tid + s].z;
-        red[tid].w += red[tid + s].w;
+    if (tid < G && c0 + tid < dp4) {
+      float4 t = red[tid];
+      for (int h = 1; h < groups; h++) {
+        const float4 v = red[h * G + tid];
+        t.x += v.x;
+        t.y += v.y;
+        t.z += v.z;
+        t.w += v.w;
       }
-      __syncthreads();
+      const float inv = 1.0f / (float)(b - a);
+      reps[(int64_t)c * dp4 + c0 + tid] = make_float4(t.x * inv, t.y * inv, t.z * inv, t.w * inv);
     }
-    if (tid == 0)
-      reps[(int64_t)c * dp4 + ch] =
-          make_float4(red[0].x * inv, red[0].y * inv, red[0].z * inv, red[0].w * inv);
     __syncthreads();
   }
 }
@@ -541,8 +551,10 @@ int launch_rep_select(const float4 *rows, int dp4, const int32_t *cand_dev,
                       int R, int trials, uint32_t *score_dev, float4 *reps,
                       int32_t *rep_rows, cudaStream_t s) {
   KNN_CUDA_TRY(cudaMemsetAsync(score_dev, 0, sizeof(uint32_t) * trials, s));
+  // 4 x 4 pairs per thread: 8 x 8 (fewer shared-memory loads per fma) took
+  // about 160 registers and measured slower on 8,192 representatives
   dim3 grid((R + 63) / 64, (R + 63) / 64, trials);
-  rep_score_kernel<<<grid, 256, 0, s>>>(rows, dp4, cand_dev, R, score_dev);
+  rep_score_kernel<4><<<grid, 256, 0, s>>>(rows, dp4, cand_dev, R, score_dev);
   KNN_LAUNCH_CHECK();
   rep_pick_kernel<<<1, 256, 0, s>>>(rows, dp4, cand_dev, R, trials, score_dev,
                                     reps, rep_rows);
