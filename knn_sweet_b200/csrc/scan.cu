@@ -135,6 +135,8 @@ struct RegTopK : TopKBase {
     reset_threshold(th0);
   }
 
+  __device__ __forceinline__ void make_room(int lane) { flush(lane); }
+
   __device__ __forceinline__ void flush(int lane) {
     if (nbuf == 0) return;
     __syncwarp();
@@ -253,6 +255,8 @@ struct SmemTopK : TopKBase {
     __syncwarp();
   }
 
+  __device__ __forceinline__ void make_room(int lane) { flush(lane); }
+
   __device__ __forceinline__ void flush(int lane) {
     if (nbuf == 0) return;
     __syncwarp();
@@ -330,6 +334,38 @@ struct SelectTopK : TopKBase {
     theta = sqrtf(key_d2(thr));
   }
 
+  // Room for more candidates while the query runs: keep every key whose
+  // squared distance is at most the k-th smallest one -- at least k keys,
+  // ties included -- found by a 32-bit selection on the keys' distance words
+  // (on data with many equal distances the 64-bit selection spends most of
+  // its passes on the index bits of the ties).  The exact k-th key is only
+  // needed at the end (flush).  Falls back to it when ties fill the buffer.
+  __device__ __forceinline__ void make_room(int lane) {
+    if (nbuf <= k) return;
+    __syncwarp();
+    const uint32_t T = warp_select_kth_u32(reinterpret_cast<const uint32_t *>(buf) + 1, 2,
+                                           nbuf, k, hist, lane);
+    int w = 0;
+    for (int b0 = 0; b0 < nbuf; b0 += 32) {
+      const int i = b0 + lane;
+      const uint64_t v = i < nbuf ? buf[i] : kKeyMax;
+      const bool keep = i < nbuf && (uint32_t)(v >> 32) <= T;
+      const unsigned bm = __ballot_sync(kFull, keep);
+      __syncwarp();
+      if (keep) buf[w + __popc(bm & ((1u << lane) - 1))] = v;
+      w += __popc(bm);
+    }
+    __syncwarp();
+    nbuf = w;
+    if (w > kCap - 32) {
+      flush(lane);
+      return;
+    }
+    merges++;
+    thr = ((uint64_t)T << 32) | 0xffffffffull;
+    theta = sqrtf(__uint_as_float(T));
+  }
+
   __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int32_t base, int lane) {
     flush(lane);
     __syncwarp();
@@ -354,7 +390,7 @@ __device__ __forceinline__ void topk_push(TK &tk, uint64_t key, int lane) {
   if (b == 0) return;
   int cnt = __popc(b);
   if (tk.nbuf + cnt > tk.cap()) {
-    tk.flush(lane);
+    tk.make_room(lane);
     pass = key < tk.thr;
     b = __ballot_sync(kFull, pass);
     cnt = __popc(b);
