@@ -367,7 +367,9 @@ struct SelectTopK : TopKBase {
   }
 
   __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int32_t base, int lane) {
-    flush(lane);
+    // up to L keys are sorted as they are (their first k are the answer);
+    // beyond that the exact k-th key is selected first
+    if (nbuf > LL) flush(lane);
     __syncwarp();
     for (int i = nbuf + lane; i < LL; i += 32) buf[i] = kKeyMax;
     __syncwarp();
