@@ -371,14 +371,40 @@ struct SelectTopK : TopKBase {
     // beyond that the exact k-th key is selected first
     if (nbuf > LL) flush(lane);
     __syncwarp();
-    for (int i = nbuf + lane; i < LL; i += 32) buf[i] = kKeyMax;
-    __syncwarp();
-    smem_bitonic_sort<LL>(buf, lane);
-    for (int t = lane; t < k; t += 32) {
-      const uint64_t key = buf[t];
-      const bool none = key == kKeyMax;
-      oi[t] = none ? -1 : key_idx(key) - base;
-      od[t] = none ? __int_as_float(0x7f800000) : (squared ? key_d2(key) : sqrtf(key_d2(key)));
+    if constexpr (LL <= 128) {
+      // sorted in registers (E keys per lane; shuffles for the cross-lane
+      // strides): lane l ends up with positions E*l .. E*l+E-1.  (At L = 256
+      // the eight keys per lane spilled under the kernel's register cap and
+      // measured slower than the shared-memory sort.)
+      constexpr int E = LL / 32;
+      uint64_t x[E];
+#pragma unroll
+      for (int j = 0; j < E; j++) {
+        const int p = j * 32 + lane;  // any order: the keys get sorted
+        x[j] = p < nbuf ? buf[p] : kKeyMax;
+      }
+      __syncwarp();
+      reg_bitonic_sort<E>(x, lane);
+#pragma unroll
+      for (int j = 0; j < E; j++) {
+        const int t = E * lane + j;
+        if (t < k) {
+          const bool none = x[j] == kKeyMax;
+          oi[t] = none ? -1 : key_idx(x[j]) - base;
+          od[t] = none ? __int_as_float(0x7f800000)
+                       : (squared ? key_d2(x[j]) : sqrtf(key_d2(x[j])));
+        }
+      }
+    } else {
+      for (int i = nbuf + lane; i < LL; i += 32) buf[i] = kKeyMax;
+      __syncwarp();
+      smem_bitonic_sort<LL>(buf, lane);
+      for (int t = lane; t < k; t += 32) {
+        const uint64_t key = buf[t];
+        const bool none = key == kKeyMax;
+        oi[t] = none ? -1 : key_idx(key) - base;
+        od[t] = none ? __int_as_float(0x7f800000) : (squared ? key_d2(key) : sqrtf(key_d2(key)));
+      }
     }
     __syncwarp();
   }
@@ -669,8 +695,10 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, L, WARPS>())
           }
         }
 #else
-        // one direction: from the lower band edge up
-        const int lo = warp_lower_bound(a.sdist + start, n_c, Dc - th - slack, lane);
+        // one direction: from the lower band edge up (no search when the band
+        // starts below the cluster's nearest member)
+        const float lo_edge = Dc - th - slack;
+        const int lo = lo_edge <= a.cmin[c] ? 0 : warp_lower_bound(a.sdist + start, n_c, lo_edge, lane);
         for (int p0 = lo; p0 < n_c; p0 += 32) {
           th = tk.theta;
           slack = tol * (2.0f * Dc + 2.0f * th);
