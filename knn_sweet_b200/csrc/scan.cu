@@ -37,69 +37,6 @@
 
 namespace knnsweet {
 
-// ---------------------------------------------------------------------------
-// Register bitonic networks over 32*E keys, blocked layout: lane l holds
-// positions E*l .. E*l+E-1.  Strides >= E pair registers of different lanes
-// (shuffle), smaller strides pair registers of the same lane.
-// ---------------------------------------------------------------------------
-// Only the within-lane strides are unrolled (their register indices must be
-// static); the cross-lane strides run as a loop, which keeps the live range
-// of the network, and so the register count, small.
-template <int E>
-__device__ __forceinline__ void reg_cross_step(uint64_t (&x)[E], int lane, int size,
-                                               int stride) {
-#pragma unroll
-  for (int j = 0; j < E; j++) {
-    const int i = E * lane + j;
-    const bool up = (i & size) == 0;
-    const bool lower = (i & stride) == 0;
-    const uint64_t o = shfl_xor64(x[j], stride / E);
-    x[j] = (lower == up) ? umin64(x[j], o) : umax64(x[j], o);
-  }
-}
-
-template <int E>
-__device__ __forceinline__ void reg_inner_steps(uint64_t (&x)[E], int lane, int size) {
-#pragma unroll
-  for (int stride = E / 2; stride > 0; stride >>= 1) {
-    if (stride < size) {
-#pragma unroll
-      for (int j = 0; j < E; j++) {
-        if ((j & stride) == 0) {
-          const int j2 = j | stride;
-          const bool up = ((E * lane + j) & size) == 0;
-          const uint64_t a = x[j], b = x[j2];
-          const bool sw = (a > b) == up;
-          x[j] = sw ? b : a;
-          x[j2] = sw ? a : b;
-        }
-      }
-    }
-  }
-}
-
-template <int E>
-__device__ __forceinline__ void reg_bitonic_sort(uint64_t (&x)[E], int lane) {
-  constexpr int L = 32 * E;
-#pragma unroll 1
-  for (int size = 2; size <= L; size <<= 1) {
-#pragma unroll 1
-    for (int stride = size >> 1; stride >= E; stride >>= 1)
-      reg_cross_step<E>(x, lane, size, stride);
-    reg_inner_steps<E>(x, lane, size);
-  }
-}
-
-// Sorts a bitonic sequence ascending (every comparison ascending: size = 2L).
-template <int E>
-__device__ __forceinline__ void reg_bitonic_merge(uint64_t (&x)[E], int lane) {
-  constexpr int L = 32 * E;
-#pragma unroll 1
-  for (int stride = L >> 1; stride >= E; stride >>= 1)
-    reg_cross_step<E>(x, lane, 2 * L, stride);
-  reg_inner_steps<E>(x, lane, 2 * L);
-}
-
 // Shared part of both top-k variants: the append buffer and the threshold.
 struct TopKBase {
   uint64_t *buf;  // append buffer (shared memory)

@@ -253,6 +253,23 @@ __device__ __forceinline__ double dist2_cols_f64(const float *__restrict__ q,
   return acc;
 }
 
+// Sorts the n <= 32E keys s[0..n) ascending in registers (padding with the
+// largest key) and writes 32E sorted keys back to s.  One warp.
+template <int E>
+__device__ __forceinline__ void sort_keys_in_registers(uint64_t *s, int n, int lane) {
+  uint64_t x[E];
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    const int p = j * 32 + lane;
+    x[j] = p < n ? s[p] : kKeyMax;
+  }
+  __syncwarp();
+  reg_bitonic_sort<E>(x, lane);
+#pragma unroll
+  for (int j = 0; j < E; j++) s[E * lane + j] = x[j];
+  __syncwarp();
+}
+
 // FP32 rounding band of a squared distance D computed by dist2_cols.
 __device__ __forceinline__ float band_eps(float D, int d) {
   return (float)(d + 4) * 5.9604645e-8f * D;
@@ -655,10 +672,27 @@ __global__ void __launch_bounds__(kTM)
         if (lane == 0) refined += (unsigned long long)m1;
         __syncwarp();
       }
-      // the k smallest keys plus every key inside the FP32 band of the k-th
-      // (compacted in place: keys[0..m2))
+      // the k smallest keys plus every key inside the FP32 band of the k-th,
+      // sorted: keys[0..m2).  Up to 128 keys are sorted directly in registers;
+      // larger sets are first cut down by a selection of the k-th key.
       int m2 = m1;
-      if (!fb && m1 > k) {
+      bool sorted = false;
+      if (!fb && m1 <= 128) {
+        if (m1 <= 32) sort_keys_in_registers<1>(keys, m1, lane);
+        else if (m1 <= 64) sort_keys_in_registers<2>(keys, m1, lane);
+        else sort_keys_in_registers<4>(keys, m1, lane);
+        sorted = true;
+        if (m1 > k) {
+          const float Dk = key_d2(keys[k - 1]);
+          const float lim2 = Dk + 2.0f * band_eps(Dk, d);
+          int w = 0;
+          for (int b0 = 0; b0 < m1; b0 += 32) {
+            const int e = b0 + lane;
+            w += __popc(__ballot_sync(kFull, e < m1 && key_d2(keys[e]) <= lim2));
+          }
+          m2 = w;
+        }
+      } else if (!fb && m1 > k) {
         const uint64_t kth = warp_select_kth(keys, m1, k, whist, lane);
         const float Dk = key_d2(kth);
         const float lim2 = Dk + 2.0f * band_eps(Dk, d);
@@ -676,12 +710,14 @@ __global__ void __launch_bounds__(kTM)
         m2 = w;
       }
       int np2 = 32;
-      while (np2 < m2) np2 <<= 1;
+      while (np2 < (sorted ? m1 : m2)) np2 <<= 1;
       if (!fb && np2 > cap) fb = true;
       if (!fb) {
-        for (int e = m2 + lane; e < np2; e += 32) keys[e] = kKeyMax;
-        __syncwarp();
-        smem_bitonic_sort_rt(keys, np2, lane);
+        if (!sorted) {
+          for (int e = m2 + lane; e < np2; e += 32) keys[e] = kKeyMax;
+          __syncwarp();
+          smem_bitonic_sort_rt(keys, np2, lane);
+        }
         if (m2 > k) {
           // keys at or above Dk - band were ranked in FP32 only to within
           // rounding: order them again by (FP64 d^2, index)
