@@ -705,8 +705,163 @@ static int launch_scan_l(const ScanArgs &a, int num_sms, cudaStream_t s) {
   return launch_scan_t<DP4, IDXROW, 1024, 4>(a, num_sms, s);
 }
 
+// ---------------------------------------------------------------------------
+// Thread-per-query scan for small k (k <= 32) and narrow rows (d <= 8).  With
+// few distances per query (k = 16 on a surface: ~200) the warp-per-query
+// scan spends most of its instructions on per-query and per-cluster overhead
+// (lane-parallel cluster tests, nearest-first ordering, 32-ary band search,
+// list merges) for bands that fill few lanes.  Here every thread walks its own
+// query, in the same order of the same candidate list, with the same pruning
+// tests and the same FP32 keys, keeping its K best keys sorted in registers
+// (K = pow2 >= k; the K-th key is the pruning bound, so for k < K the bound is
+// looser but the first k keys are still the k nearest).  The 32 queries of a
+// warp are consecutive slots, mostly of one query cluster, so they walk
+// similar lists.
+// ---------------------------------------------------------------------------
+template <int K>
+struct ThreadTopK {
+  uint64_t key[K];  // ascending; kKeyMax = empty
+  __device__ __forceinline__ void reset() {
+#pragma unroll
+    for (int j = 0; j < K; j++) key[j] = kKeyMax;
+  }
+  // inserts v, which must be smaller than key[K-1]
+  __device__ __forceinline__ void insert(uint64_t v) {
+#pragma unroll
+    for (int j = K - 1; j > 0; j--) {
+      const uint64_t prev = key[j - 1];
+      key[j] = prev > v ? prev : (key[j] > v ? v : key[j]);
+    }
+    key[0] = key[0] > v ? v : key[0];
+  }
+};
+
+template <int DP4, bool IDXROW, int K>
+__global__ void __launch_bounds__(256)
+    thread_scan_kernel(const ScanArgs a) {
+  __shared__ unsigned long long blk_ctr[5];
+  if (threadIdx.x < 5) blk_ctr[threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t nslots = a.slot_list ? (int64_t)*a.slot_count : a.m;
+  unsigned evals = 0, visited = 0, pruned = 0, pushed = 0;
+  if (t < nslots) {
+    const int64_t slot = a.slot_list ? (int64_t)a.slot_list[t] : t;
+    const int64_t q = a.qorder[slot];
+    const int qc = a.slot_cl[slot];
+    const float tol = bound_tol(a.d);
+    QueryRow<DP4, IDXROW> qr;
+    qr.load(a.qrows, q, DP4, nullptr);
+    ThreadTopK<K> tk;
+    tk.reset();
+    float theta = a.theta0[qc];
+    // admits every d^2 <= theta0^2, whatever the index
+    const uint64_t thr0 = ((uint64_t)__float_as_uint(theta * theta) << 32) | 0xffffffffull;
+    const int nr = a.rlen[qc];
+    const int32_t *rl = a.rlist + (a.rl_base ? a.rl_base[qc] : (int64_t)qc * a.Rs);
+    for (int j = 0; j < nr; j++) {
+      const int c = rl[j];
+      const float D = sqrtf(qr.dist2(a.sreps + (int64_t)c * DP4, DP4));
+      float slack = tol * (2.0f * D + 2.0f * theta);
+      const float cmin = a.cmin[c];
+      if (D - a.cmax[c] > theta + slack || D + theta + slack < cmin) {
+        pruned++;
+        continue;
+      }
+      visited++;
+      const int start = a.soff[c], n_c = a.soff[c + 1] - start;
+      const float *sd = a.sdist + start;
+      // first member of the band [D - theta, D + theta] (with slack)
+      const float lo_edge = D - theta - slack;
+      int p = 0;
+      if (lo_edge > cmin) {
+        int hi = n_c;
+        while (p < hi) {
+          const int md = (p + hi) >> 1;
+          if (sd[md] < lo_edge) p = md + 1;
+          else hi = md;
+        }
+      }
+      for (; p < n_c; p++) {
+        if (sd[p] > D + theta + slack) break;
+        float4 row[DP4];
+#pragma unroll
+        for (int cc = 0; cc < DP4; cc++) row[cc] = a.srows[(int64_t)(start + p) * DP4 + cc];
+        int32_t idx = 0;
+        const float v = qr.dist2_member(row, &idx);
+        evals++;
+        if (!IDXROW) idx = a.sidx[start + p];
+        const uint64_t key = make_key(v, idx);
+        if (key < thr0 && key < tk.key[K - 1]) {
+          tk.insert(key);
+          pushed++;
+          if (tk.key[K - 1] != kKeyMax) {
+            theta = sqrtf(key_d2(tk.key[K - 1]));
+            slack = tol * (2.0f * D + 2.0f * theta);
+          }
+        }
+      }
+    }
+    int32_t *oi = a.out_idx + q * a.k;
+    float *od = a.out_dist + q * a.k;
+    const int32_t base = a.qc_ref_base ? (int32_t)a.qc_ref_base[qc] : 0;
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+      if (j < a.k) {
+        const uint64_t key = tk.key[j];
+        const bool none = key == kKeyMax;
+        oi[j] = none ? -1 : key_idx(key) - base;
+        const float d2 = key_d2(key);
+        od[j] = none ? __int_as_float(0x7f800000) : (a.squared ? d2 : sqrtf(d2));
+      }
+    }
+  }
+  if (a.counters) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      evals += __shfl_xor_sync(kFull, evals, o);
+      visited += __shfl_xor_sync(kFull, visited, o);
+      pruned += __shfl_xor_sync(kFull, pruned, o);
+      pushed += __shfl_xor_sync(kFull, pushed, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(&blk_ctr[0], (unsigned long long)evals);
+      atomicAdd(&blk_ctr[1], (unsigned long long)visited);
+      atomicAdd(&blk_ctr[2], (unsigned long long)pruned);
+      atomicAdd(&blk_ctr[3], (unsigned long long)pushed);
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) atomicAdd(a.counters + threadIdx.x, blk_ctr[threadIdx.x]);
+  }
+}
+
+template <int DP4, bool IDXROW>
+static int launch_thread_scan(const ScanArgs &a, cudaStream_t s) {
+  const int blocks = (int)((a.m + 255) / 256);
+  auto go = [&](auto kern) -> int {
+    kern<<<blocks, 256, 0, s>>>(a);
+    KNN_LAUNCH_CHECK();
+    return KNN_OK;
+  };
+  if (a.k <= 1) return go(thread_scan_kernel<DP4, IDXROW, 1>);
+  if (a.k <= 2) return go(thread_scan_kernel<DP4, IDXROW, 2>);
+  if (a.k <= 4) return go(thread_scan_kernel<DP4, IDXROW, 4>);
+  if (a.k <= 8) return go(thread_scan_kernel<DP4, IDXROW, 8>);
+  if (a.k <= 16) return go(thread_scan_kernel<DP4, IDXROW, 16>);
+  return go(thread_scan_kernel<DP4, IDXROW, 32>);
+}
+
+#ifndef KNN_THREAD_SCAN_MAX_K
+#define KNN_THREAD_SCAN_MAX_K 32
+#endif
+
 int launch_scan(const ScanArgs &a, int num_sms, cudaStream_t s) {
   if (a.m == 0) return KNN_OK;
+  if (a.k <= KNN_THREAD_SCAN_MAX_K && (a.dp4_tmpl == 1 || a.dp4_tmpl == 2)) {
+    if (a.dp4_tmpl == 1)
+      return a.idx_in_row ? launch_thread_scan<1, true>(a, s) : launch_thread_scan<1, false>(a, s);
+    return a.idx_in_row ? launch_thread_scan<2, true>(a, s) : launch_thread_scan<2, false>(a, s);
+  }
   switch (a.dp4_tmpl) {
     case 1: return a.idx_in_row ? launch_scan_l<1, true>(a, num_sms, s)
                                 : launch_scan_l<1, false>(a, num_sms, s);
