@@ -579,6 +579,7 @@ int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t 
   a.rlist = rlist;
   a.rlen = rlen;
   a.Rs = Rs;
+  a.n_ref = n;
   a.out_idx = out_idx;
   a.out_dist = out_dist;
   a.work_counter = ctr;

@@ -482,6 +482,7 @@ int batched_impl(const float *q, const int64_t *qoff_h, const float *r, const in
       a.rl_base = rl_base;
       a.qc_ref_base = qc_ref_base;
       a.Rs = S.Rtot;
+      a.n_ref = S.total;
       a.out_idx = out_idx;
       a.out_dist = out_dist;
       a.work_counter = ctr;

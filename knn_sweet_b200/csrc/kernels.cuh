@@ -31,6 +31,8 @@ struct ScanArgs {
   const int32_t *slot_list;    // optional: scan only these slots ...
   const unsigned *slot_count;  // ... *slot_count of them (device count)
   int Rs;
+  int64_t n_ref;            // reference points (0: unknown); with Rs it gives
+                            // the mean cluster size the scan variant is chosen by
   int32_t *out_idx;         // m x k
   float *out_dist;          // m x k
   unsigned long long *work_counter;  // zeroed before launch

@@ -857,7 +857,13 @@ static int launch_thread_scan(const ScanArgs &a, cudaStream_t s) {
 
 int launch_scan(const ScanArgs &a, int num_sms, cudaStream_t s) {
   if (a.m == 0) return KNN_OK;
-  if (a.k <= KNN_THREAD_SCAN_MAX_K && (a.dp4_tmpl == 1 || a.dp4_tmpl == 2)) {
+  // thread per query: small k, rows of at most 8 floats, and short bands (at
+  // most 128 points per cluster on average).  Measured: 4,096 surface clouds
+  // (~70-100 points per cluster, k = 16) 143 -> 67 ms; a dense 3-D set with
+  // ~300 points per cluster at k = 32 2.7 -> 4.3 ms (slower); d = 16 and 32
+  // slower too.
+  const bool short_bands = a.n_ref > 0 && a.Rs > 0 && a.n_ref <= 128 * (int64_t)a.Rs;
+  if (a.k <= KNN_THREAD_SCAN_MAX_K && short_bands && (a.dp4_tmpl == 1 || a.dp4_tmpl == 2)) {
     if (a.dp4_tmpl == 1)
       return a.idx_in_row ? launch_thread_scan<1, true>(a, s) : launch_thread_scan<1, false>(a, s);
     return a.idx_in_row ? launch_thread_scan<2, true>(a, s) : launch_thread_scan<2, false>(a, s);
