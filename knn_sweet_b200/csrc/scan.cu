@@ -570,26 +570,55 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, L, WARPS>())
       // distance) or, with KNN_ORDER_BY_D, nearest d(q, Rs) first
       unsigned amask = __ballot_sync(kFull, alive);
       float dkey = alive ? D : __int_as_float(0x7f800000);
-      while (amask) {
-        int src = __ffs(amask) - 1;
-#if KNN_ORDER_BY_D
-        if (amask & (amask - 1)) {
-          float mv = dkey;
-          int ml = lane;
+      // Visit order: nearest d(q, Rs) first.  Narrow rows sort the batch once
+      // (bitonic network over the 32 lanes, ties to the lower lane: less work
+      // per visited cluster); wider rows pick the nearest remaining cluster
+      // by a warp arg-min per visit (measured faster there).
+      constexpr bool kSortBatch = KNN_ORDER_BY_D != 0 && DP4 >= 1 && DP4 <= 2;
+      float sv = dkey;
+      int sl = lane;
+      if constexpr (kSortBatch) {
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            const float ov = __shfl_xor_sync(kFull, mv, o);
-            const int ol = __shfl_xor_sync(kFull, ml, o);
-            if (ov < mv || (ov == mv && ol < ml)) {
-              mv = ov;
-              ml = ol;
+        for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+          for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const float ov = __shfl_xor_sync(kFull, sv, stride);
+            const int ol = __shfl_xor_sync(kFull, sl, stride);
+            const bool other_less = ov < sv || (ov == sv && ol < sl);
+            const bool keep_min = ((lane & stride) == 0) == ((lane & size) == 0);
+            if (other_less == keep_min) {
+              sv = ov;
+              sl = ol;
             }
           }
-          src = ml;
         }
-        if (lane == src) dkey = __int_as_float(0x7f800000);
+      }
+      const int nalive = __popc(amask);
+      for (int rank = 0; rank < nalive; rank++) {
+        int src;
+        if constexpr (kSortBatch) {
+          src = __shfl_sync(kFull, sl, rank);
+        } else {
+          src = __ffs(amask) - 1;
+#if KNN_ORDER_BY_D
+          if (amask & (amask - 1)) {
+            float mv = dkey;
+            int ml = lane;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+              const float ov = __shfl_xor_sync(kFull, mv, o);
+              const int ol = __shfl_xor_sync(kFull, ml, o);
+              if (ov < mv || (ov == mv && ol < ml)) {
+                mv = ov;
+                ml = ol;
+              }
+            }
+            src = ml;
+          }
+          if (lane == src) dkey = __int_as_float(0x7f800000);
 #endif
-        amask &= ~(1u << src);
+          amask &= ~(1u << src);
+        }
         const float Dc = __shfl_sync(kFull, D, src);
         const int c = __shfl_sync(kFull, rs, src);
         float th = tk.theta;
