@@ -3,10 +3,10 @@
 // For rows wide enough to be a dense contraction (d >= 16) the assignment of
 // every point to its nearest representative (findQCluster / findTCluster,
 // src/knnjoin.cu:64-97, over the cuBLAS distance matrix of knnjoin.cu:270-342)
-// is an n x R x d GEMM with an arg-min epilogue:
-//     argmin_j  |r_j|^2 - 2 p . r_j
+// is an n x R x d GEMM with an arg-max epilogue:
+//     argmax_j  p . r_j - |r_j|^2 / 2
 // computed from BF16-rounded points and representatives with FP32 accumulation
-// in TMEM.  The choice only has to be approximately nearest: the pruning
+// in TMEM; the norm term rides in three extra contraction columns.  The choice only has to be approximately nearest: the pruning
 // bounds need the exact distance to whichever representative is chosen, and
 // that distance is recomputed in FP32 afterwards (exact_rep_dist_kernel).
 //
@@ -15,7 +15,7 @@
 // of TN = 128 representatives (pre-converted once, contiguous) arrive by bulk
 // asynchronous copy; thread 0 issues KD/16 MMAs (M = 128, N = TN, K = 16)
 // per tile into one of two TMEM accumulators and commits to an mbarrier; the
-// warps read the rows back (tcgen05.ld 32x32b) and keep a running arg-min per
+// warps read the rows back (tcgen05.ld 32x32b) and keep a running arg-max per
 // row while the next tile's MMA runs.  Every wait is bounded; on timeout the
 // CTA flags the error, frees its TMEM and returns.
 #include <cuda_bf16.h>
@@ -31,72 +31,87 @@ constexpr int kTileM = 128;  // points per CTA (TMEM lanes)
 constexpr int kTileN = 256;  // representatives per MMA (TMEM columns)
 }  // namespace
 
-// Representatives -> BF16 tiles of kTileN rows in the core-matrix layout, and
-// their squared norms (of the rounded values); padding rows get norm +inf so
-// they never win the arg-min.
+// Representatives -> BF16 tiles of kTileN rows in the core-matrix layout.
+// Columns d, d+1 and d+2 carry the squared norm of the BF16-rounded row,
+// split into three BF16 parts whose sum is the FP32 norm (8 significant bits
+// each); the points carry -0.5 there, so the MMA yields p.r - |r|^2 / 2 and
+// the nearest representative is its arg-max.  Padding rows carry the largest
+// finite BF16 value as the norm: they never win.
 __global__ void reps_to_bf16_tiles_kernel(const float4 *__restrict__ reps, int R, int dp4,
                                           int d, int KD, int Rpad,
-                                          __nv_bfloat16 *__restrict__ tiles,
-                                          float *__restrict__ rnorm) {
+                                          __nv_bfloat16 *__restrict__ tiles) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= Rpad) return;
   unsigned char *tile = reinterpret_cast<unsigned char *>(tiles) +
                         (size_t)(r / kTileN) * tc::tile_bytes(kTileN, KD);
   const int rr = r % kTileN;
-  float nrm = 0.0f;
+  auto coord = [&](int k) -> float {
+    const float4 c = reps[(size_t)r * dp4 + (k >> 2)];
+    return (k & 3) == 0 ? c.x : (k & 3) == 1 ? c.y : (k & 3) == 2 ? c.z : c.w;
+  };
+  __nv_bfloat16 part[3];
+  if (r < R) {
+    float nrm = 0.0f;
+    for (int k = 0; k < d; k++) {
+      const float xr = __bfloat162float(__float2bfloat16_rn(coord(k)));
+      nrm = __fmaf_rn(xr, xr, nrm);
+    }
+    // each remainder is exact in FP32: the part is the remainder rounded
+#pragma unroll
+    for (int t = 0; t < 3; t++) {
+      part[t] = __float2bfloat16_rn(nrm);
+      nrm -= __bfloat162float(part[t]);
+    }
+  } else {
+    part[0] = __ushort_as_bfloat16(0x7f7f);
+    part[1] = part[2] = __float2bfloat16_rn(0.0f);
+  }
   for (int k0 = 0; k0 < KD; k0 += 8) {
     __align__(16) __nv_bfloat16 v[8];
 #pragma unroll
     for (int e = 0; e < 8; e++) {
       const int k = k0 + e;
-      float x = 0.0f;
-      if (r < R && k < d) {
-        const float4 c = reps[(size_t)r * dp4 + (k >> 2)];
-        x = (k & 3) == 0 ? c.x : (k & 3) == 1 ? c.y : (k & 3) == 2 ? c.z : c.w;
-      }
-      v[e] = __float2bfloat16_rn(x);
-      const float xr = __bfloat162float(v[e]);
-      nrm = __fmaf_rn(xr, xr, nrm);
+      v[e] = k >= d && k < d + 3 ? part[k - d]
+             : (r < R && k < d)  ? __float2bfloat16_rn(coord(k))
+                                 : __float2bfloat16_rn(0.0f);
     }
     *reinterpret_cast<uint4 *>(tile + tc::tile_offset(rr, k0, KD)) =
         *reinterpret_cast<const uint4 *>(v);
   }
-  rnorm[r] = r < R ? nrm : __int_as_float(0x7f800000);
 }
 
 // Pipelined arg-min: 256 threads (8 warps) own 128 points.  The
 // representative tiles (pre-converted, contiguous) stream through two
 // shared-memory buffers by 1-D bulk asynchronous copies that complete on an
 // mbarrier transaction count; two TMEM accumulators of TN columns let the MMA
-// of tile j+1 run while the epilogue reads tile j.  Warps w and w+4 read the
-// same 32 TMEM lanes (rows) and split the TN columns; each thread keeps four
-// independent running minima (column c goes to chain c % 4), merged by
-// (value, index) at the end so ties still go to the lowest index.
-// dynamic shared memory: A tile, 2 B tiles, 2 x TN norms, 4 mbarriers,
-// TMEM slot, 128 (value, index) pairs
+// of tile j+1 run while the epilogue reads tile j.  The accumulator holds
+// p.r - |r|^2 / 2 (norm columns folded into the contraction), so the
+// epilogue is a bare arg-max.  Warps w and w+4 read the same 32 TMEM lanes
+// (rows) and split the TN columns; each thread keeps four independent running
+// maxima (column c goes to chain c % 4), merged by (value, index) at the end
+// so ties still go to the lowest index.
+// dynamic shared memory: A tile, 2 B tiles, 4 mbarriers, TMEM slot, 128
+// (value, index) pairs
 __global__ void __launch_bounds__(256, 1)
     assign_tc_kernel(const float4 *__restrict__ rows, int64_t n, int dp4, int d, int KD, int TN,
-                     const __nv_bfloat16 *__restrict__ rep_tiles,
-                     const float *__restrict__ rnorm, int ntiles,
+                     const __nv_bfloat16 *__restrict__ rep_tiles, int ntiles,
                      int32_t *__restrict__ cl, int *__restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const size_t a_bytes = tc::tile_bytes(kTileM, KD), b_bytes = tc::tile_bytes(TN, KD);
   unsigned char *sa = smem;
   unsigned char *sb0 = sa + a_bytes, *sb1 = sb0 + b_bytes;
-  float *sn0 = reinterpret_cast<float *>(sb1 + b_bytes), *sn1 = sn0 + TN;
   auto sb = [&](int b) { return b ? sb1 : sb0; };
-  auto sn = [&](int b) { return b ? sn1 : sn0; };
-  uint64_t *full = reinterpret_cast<uint64_t *>(sn1 + TN);  // 2: copies landed
+  uint64_t *full = reinterpret_cast<uint64_t *>(sb1 + b_bytes);  // 2: copies landed
   uint64_t *done = full + 2;                                    // 2: MMA finished
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 2);
-  float *pv = reinterpret_cast<float *>(tmem_slot + 4);         // 128 partial minima
+  float *pv = reinterpret_cast<float *>(tmem_slot + 4);         // 128 partial maxima
   int *pi = reinterpret_cast<int *>(pv + kTileM);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int quad = warp & 3, half = warp >> 2;
   const int64_t row0 = (int64_t)blockIdx.x * kTileM;
   const uint32_t ncols = 2u * (uint32_t)TN;  // 256 or 512, a power of two
-  const uint32_t tile_tx = (uint32_t)(b_bytes + (size_t)TN * sizeof(float));
+  const uint32_t tile_tx = (uint32_t)b_bytes;
 
   if (warp == 0) tc::tmem_alloc(tmem_slot, ncols);
   if (tid == 0) {
@@ -113,7 +128,6 @@ __global__ void __launch_bounds__(256, 1)
       tc::mbar_arrive_expect_tx(full + j, tile_tx);
       tc::bulk_copy_g2s(sb(j), reinterpret_cast<const unsigned char *>(rep_tiles) + (size_t)j * b_bytes,
                         (uint32_t)b_bytes, full + j);
-      tc::bulk_copy_g2s(sn(j), rnorm + (size_t)j * TN, (uint32_t)(TN * sizeof(float)), full + j);
     }
   }
   // points -> BF16 core-matrix tile
@@ -128,6 +142,8 @@ __global__ void __launch_bounds__(256, 1)
       if (gr < n && k < d) {
         const float4 c = rows[gr * dp4 + (k >> 2)];
         x = (k & 3) == 0 ? c.x : (k & 3) == 1 ? c.y : (k & 3) == 2 ? c.z : c.w;
+      } else if (gr < n && k < d + 3) {
+        x = -0.5f;  // times the representative's norm columns
       }
       v[e] = __float2bfloat16_rn(x);
     }
@@ -163,7 +179,7 @@ __global__ void __launch_bounds__(256, 1)
   int bidx[4];
 #pragma unroll
   for (int c = 0; c < 4; c++) {
-    best[c] = __int_as_float(0x7f800000);
+    best[c] = __int_as_float(0xff800000);
     bidx[c] = 0;
   }
   const int cbeg = half * (TN / 2);
@@ -175,7 +191,6 @@ __global__ void __launch_bounds__(256, 1)
     if (!ok) break;
     tc::fence_after_sync();
     const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * TN + cbeg);
-    const float *nrm = sn(b) + cbeg;
     const int jbase = j * TN + cbeg;
 #pragma unroll 1
     for (int c0 = 0; c0 < TN / 2; c0 += 32) {
@@ -183,31 +198,28 @@ __global__ void __launch_bounds__(256, 1)
       tc::tmem_ld_32x32(lane_base + (uint32_t)c0, acc);
 #pragma unroll
       for (int jj = 0; jj < 32; jj++) {
-        const float v = __fmaf_rn(-2.0f, acc[jj], nrm[c0 + jj]);
-        if (v < best[jj & 3]) {
-          best[jj & 3] = v;
+        if (acc[jj] > best[jj & 3]) {
+          best[jj & 3] = acc[jj];
           bidx[jj & 3] = jbase + c0 + jj;
         }
       }
     }
     tc::fence_before_sync();
-    __syncthreads();  // accumulator b, tile b and its norms are free again
+    __syncthreads();  // accumulator b and tile b are free again
     if (tid == 0 && j + 2 < ntiles) {
       tc::fence_proxy_async_smem();
       tc::mbar_arrive_expect_tx(full + b, tile_tx);
       tc::bulk_copy_g2s(sb(b), reinterpret_cast<const unsigned char *>(rep_tiles) +
                                    (size_t)(j + 2) * b_bytes,
                         (uint32_t)b_bytes, full + b);
-      tc::bulk_copy_g2s(sn(b), rnorm + (size_t)(j + 2) * TN, (uint32_t)(TN * sizeof(float)),
-                        full + b);
     }
   }
-  // merge the chains: smallest value, then lowest index
+  // merge the chains: largest value, then lowest index
   float bv = best[0];
   int bi = bidx[0];
 #pragma unroll
   for (int c = 1; c < 4; c++)
-    if (best[c] < bv || (best[c] == bv && bidx[c] < bi)) {
+    if (best[c] > bv || (best[c] == bv && bidx[c] < bi)) {
       bv = best[c];
       bi = bidx[c];
     }
@@ -220,7 +232,7 @@ __global__ void __launch_bounds__(256, 1)
   if (half == 0) {
     const float ov = pv[rrow];
     const int oi = pi[rrow];
-    if (ov < bv || (ov == bv && oi < bi)) {
+    if (ov > bv || (ov == bv && oi < bi)) {
       bv = ov;
       bi = oi;
     }
@@ -250,30 +262,28 @@ __global__ void exact_rep_dist_kernel(const float4 *__restrict__ rows, int64_t n
 
 bool assign_tc_supported(int d) { return d >= 16 && d <= 256; }
 
+// contraction depth: the coordinates and three norm columns, in MMA steps
+static int assign_kd(int d) { return (d + 3 + 15) / 16 * 16; }
+
 size_t assign_tc_scratch_bytes(int R, int d) {
-  const int KD = (d + 15) / 16 * 16;
   const int Rpad = (R + kTileN - 1) / kTileN * kTileN;
-  return tc::tile_bytes(Rpad, KD) + 256 + (size_t)Rpad * sizeof(float) + 256 + 256;
+  return tc::tile_bytes(Rpad, assign_kd(d)) + 256;
 }
 
 int launch_assign_tc(const float4 *rows, int64_t n, int dp4, int d, const float4 *reps, int R,
                      void *scratch, int32_t *cl, float *dr, int *err, cudaStream_t s) {
   if (n == 0) return KNN_OK;
-  const int KD = (d + 15) / 16 * 16;
+  const int KD = assign_kd(d);
   const int Rpad = (R + kTileN - 1) / kTileN * kTileN;
-  unsigned char *p = static_cast<unsigned char *>(scratch);
-  __nv_bfloat16 *tiles = reinterpret_cast<__nv_bfloat16 *>(p);
-  float *rnorm = reinterpret_cast<float *>(p + ((tc::tile_bytes(Rpad, KD) + 255) & ~(size_t)255));
-  reps_to_bf16_tiles_kernel<<<(Rpad + 127) / 128, 128, 0, s>>>(reps, R, dp4, d, KD, Rpad, tiles,
-                                                               rnorm);
+  __nv_bfloat16 *tiles = static_cast<__nv_bfloat16 *>(scratch);
+  reps_to_bf16_tiles_kernel<<<(Rpad + 127) / 128, 128, 0, s>>>(reps, R, dp4, d, KD, Rpad, tiles);
   KNN_LAUNCH_CHECK();
   // representative tiles of 128 rows: a CTA then holds 256 TMEM columns and
   // two CTAs share an SM, whose warps hide each other's epilogue latency
   // (measured faster than 256-row tiles with one CTA per SM)
   const int TN = kTileN / 2;
   const size_t need = tc::tile_bytes(kTileM, KD) + 2 * tc::tile_bytes(TN, KD) +
-                      2 * (size_t)TN * sizeof(float) + 4 * sizeof(uint64_t) + 16 +
-                      (size_t)kTileM * 8;
+                      4 * sizeof(uint64_t) + 16 + (size_t)kTileM * 8;
   // a CTA holds 2 x TN TMEM columns: with TN = 256 that is all 512, so at
   // most one CTA per SM (over 114 KB each), with TN = 128 at most two
   const size_t smem = std::max<size_t>(need, TN == kTileN ? 116 * 1024 : 80 * 1024);
@@ -283,7 +293,7 @@ int launch_assign_tc(const float4 *rows, int64_t n, int dp4, int d, const float4
                                     cudaFuncAttributePreferredSharedMemoryCarveout,
                                     cudaSharedmemCarveoutMaxShared));
   const int64_t blocks = (n + kTileM - 1) / kTileM;
-  assign_tc_kernel<<<(unsigned)blocks, 256, smem, s>>>(rows, n, dp4, d, KD, TN, tiles, rnorm,
+  assign_tc_kernel<<<(unsigned)blocks, 256, smem, s>>>(rows, n, dp4, d, KD, TN, tiles,
                                                        Rpad / TN, cl, err);
   KNN_LAUNCH_CHECK();
   exact_rep_dist_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 32), 256, 0, s>>>(
