@@ -80,19 +80,27 @@ __global__ void reps_to_bf16_tiles_kernel(const float4 *__restrict__ reps, int R
   }
 }
 
-// Pipelined arg-min: 256 threads (8 warps) own 128 points.  The
-// representative tiles (pre-converted, contiguous) stream through two
-// shared-memory buffers by 1-D bulk asynchronous copies that complete on an
-// mbarrier transaction count; two TMEM accumulators of TN columns let the MMA
-// of tile j+1 run while the epilogue reads tile j.  The accumulator holds
+// Warp-specialised arg-max: warps 0-7 (the epilogue) own 128 points, warp 8
+// (the producer) streams the representative tiles (pre-converted,
+// contiguous) through two shared-memory buffers by 1-D bulk asynchronous
+// copies that complete on an mbarrier transaction count, and issues the MMAs
+// into two TMEM accumulators of TN columns.  The accumulator holds
 // p.r - |r|^2 / 2 (norm columns folded into the contraction), so the
-// epilogue is a bare arg-max.  Warps w and w+4 read the same 32 TMEM lanes
-// (rows) and split the TN columns; each thread keeps four independent running
-// maxima (column c goes to chain c % 4), merged by (value, index) at the end
-// so ties still go to the lowest index.
-// dynamic shared memory: A tile, 2 B tiles, 4 mbarriers, TMEM slot, 128
-// (value, index) pairs
-__global__ void __launch_bounds__(256, 1)
+// epilogue is a bare arg-max.  Handshakes, all mbarriers, no CTA barrier in
+// the loop:
+//   full[b]   copy of the tile in buffer b landed        (producer waits)
+//   done[b]   MMA into accumulator b finished            (both wait)
+//   empty[b]  8 epilogue warps finished reading b        (producer waits)
+// Warps w and w+4 read the same 32 TMEM lanes (rows) and split the TN
+// columns; each thread keeps four independent running maxima (column c goes
+// to chain c % 4), merged by (value, index) at the end so ties still go to
+// the lowest index.  Any wait that gives up raises a shared abort flag that
+// the other warps check before their next wait.
+// dynamic shared memory: A tile, 2 B tiles, 6 mbarriers, TMEM slot, abort
+// flag, 128 (value, index) pairs
+constexpr int kAssignThreads = 288;
+
+__global__ void __launch_bounds__(kAssignThreads, 1)
     assign_tc_kernel(const float4 *__restrict__ rows, int64_t n, int dp4, int d, int KD, int TN,
                      const __nv_bfloat16 *__restrict__ rep_tiles, int ntiles,
                      int32_t *__restrict__ cl, int *__restrict__ err) {
@@ -101,35 +109,37 @@ __global__ void __launch_bounds__(256, 1)
   unsigned char *sa = smem;
   unsigned char *sb0 = sa + a_bytes, *sb1 = sb0 + b_bytes;
   auto sb = [&](int b) { return b ? sb1 : sb0; };
-  uint64_t *full = reinterpret_cast<uint64_t *>(sb1 + b_bytes);  // 2: copies landed
-  uint64_t *done = full + 2;                                    // 2: MMA finished
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 2);
-  float *pv = reinterpret_cast<float *>(tmem_slot + 4);         // 128 partial maxima
+  uint64_t *full = reinterpret_cast<uint64_t *>(sb1 + b_bytes);
+  uint64_t *done = full + 2;
+  uint64_t *empty = done + 2;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(empty + 2);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+  float *pv = reinterpret_cast<float *>(tmem_slot + 4);  // 128 partial maxima
   int *pi = reinterpret_cast<int *>(pv + kTileM);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int quad = warp & 3, half = warp >> 2;
   const int64_t row0 = (int64_t)blockIdx.x * kTileM;
   const uint32_t ncols = 2u * (uint32_t)TN;  // 256 or 512, a power of two
-  const uint32_t tile_tx = (uint32_t)b_bytes;
+  const unsigned char *tiles_g = reinterpret_cast<const unsigned char *>(rep_tiles);
 
   if (warp == 0) tc::tmem_alloc(tmem_slot, ncols);
   if (tid == 0) {
     for (int i = 0; i < 2; i++) {
       tc::mbar_init(full + i, 1);
       tc::mbar_init(done + i, 1);
+      tc::mbar_init(empty + i, 8);
     }
+    *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  const bool producer = warp == 8 && lane == 0;
   // first two representative tiles in flight while the points are staged
-  if (tid == 0) {
+  if (producer)
     for (int j = 0; j < 2 && j < ntiles; j++) {
-      tc::mbar_arrive_expect_tx(full + j, tile_tx);
-      tc::bulk_copy_g2s(sb(j), reinterpret_cast<const unsigned char *>(rep_tiles) + (size_t)j * b_bytes,
-                        (uint32_t)b_bytes, full + j);
+      tc::mbar_arrive_expect_tx(full + j, (uint32_t)b_bytes);
+      tc::bulk_copy_g2s(sb(j), tiles_g + (size_t)j * b_bytes, (uint32_t)b_bytes, full + j);
     }
-  }
   // points -> BF16 core-matrix tile
   for (int t = tid; t < kTileM * (KD / 8); t += blockDim.x) {
     const int r = t / (KD / 8), k0 = (t % (KD / 8)) * 8;
@@ -155,100 +165,124 @@ __global__ void __launch_bounds__(256, 1)
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = *tmem_slot;
-  const uint32_t idesc = tc::make_idesc_bf16(kTileM, TN);
-  const uint32_t a_base = tc::smem_u32(sa);
-  const uint32_t sbo = (uint32_t)KD * 16;
-  bool ok = true;
-  // MMA of tile j into accumulator j & 1 (thread 0), after its copy landed
-  auto issue = [&](int j) -> bool {
-    const int b = j & 1;
-    if (!tc::mbar_wait(full + b, (uint32_t)((j >> 1) & 1))) return false;
-    tc::fence_after_sync();
-    const uint32_t b_base = tc::smem_u32(sb(b));
-    for (int st = 0; st < KD / 16; st++) {
-      const uint64_t ad = tc::make_desc(a_base + 256u * st, 128u, sbo);
-      const uint64_t bd = tc::make_desc(b_base + 256u * st, 128u, sbo);
-      tc::mma_bf16(tmem + (uint32_t)(b * TN), ad, bd, idesc, st > 0);
-    }
-    tc::mma_commit(done + b);
-    return true;
-  };
-  bool issued = true;
-  if (tid == 0 && ntiles > 0) issued = issue(0);
-  float best[4];
-  int bidx[4];
-#pragma unroll
-  for (int c = 0; c < 4; c++) {
-    best[c] = __int_as_float(0xff800000);
-    bidx[c] = 0;
-  }
-  const int cbeg = half * (TN / 2);
-  for (int j = 0; j < ntiles; j++) {
-    const int b = j & 1;
-    if (tid == 0 && issued && j + 1 < ntiles) issued = issue(j + 1);
-    bool w = tc::mbar_wait(done + b, (uint32_t)((j >> 1) & 1));
-    ok = __syncthreads_and(w && (tid != 0 || issued)) != 0;
-    if (!ok) break;
-    tc::fence_after_sync();
-    const uint32_t lane_base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * TN + cbeg);
-    const int jbase = j * TN + cbeg;
-#pragma unroll 1
-    for (int c0 = 0; c0 < TN / 2; c0 += 32) {
-      float acc[32];
-      tc::tmem_ld_32x32(lane_base + (uint32_t)c0, acc);
-#pragma unroll
-      for (int jj = 0; jj < 32; jj++) {
-        if (acc[jj] > best[jj & 3]) {
-          best[jj & 3] = acc[jj];
-          bidx[jj & 3] = jbase + c0 + jj;
+
+  float bv = __int_as_float(0xff800000);
+  int bi = 0;
+  if (warp == 8) {
+    if (producer) {
+      const uint32_t idesc = tc::make_idesc_bf16(kTileM, TN);
+      const uint32_t a_base = tc::smem_u32(sa);
+      const uint32_t sbo = (uint32_t)KD * 16;
+      int copies = ntiles < 2 ? ntiles : 2, mmas = 0;
+      // MMA of tile j into accumulator j & 1, once its copy landed and the
+      // epilogue released the accumulator (tile j - 2)
+      auto issue = [&](int j) -> bool {
+        const int b = j & 1;
+        if (j >= 2 && !tc::mbar_wait(empty + b, (uint32_t)(((j - 2) >> 1) & 1))) return false;
+        if (!tc::mbar_wait(full + b, (uint32_t)((j >> 1) & 1))) return false;
+        tc::fence_after_sync();
+        const uint32_t b_base = tc::smem_u32(sb(b));
+        for (int st = 0; st < KD / 16; st++) {
+          const uint64_t ad = tc::make_desc(a_base + 256u * st, 128u, sbo);
+          const uint64_t bd = tc::make_desc(b_base + 256u * st, 128u, sbo);
+          tc::mma_bf16(tmem + (uint32_t)(b * TN), ad, bd, idesc, st > 0);
+        }
+        tc::mma_commit(done + b);
+        mmas = j + 1;
+        return true;
+      };
+      bool ok = ntiles == 0 || issue(0);
+      for (int j = 0; ok && j < ntiles; j++) {
+        if (*abort_flag) { ok = false; break; }
+        // queue MMA j + 1 behind MMA j, then refill buffer j & 1 with tile
+        // j + 2 once MMA j has read it
+        if (j + 1 < ntiles && !issue(j + 1)) { ok = false; break; }
+        if (j + 2 < ntiles) {
+          const int b = j & 1;
+          if (!tc::mbar_wait(done + b, (uint32_t)((j >> 1) & 1))) { ok = false; break; }
+          tc::mbar_arrive_expect_tx(full + b, (uint32_t)b_bytes);
+          tc::bulk_copy_g2s(sb(b), tiles_g + (size_t)(j + 2) * b_bytes, (uint32_t)b_bytes,
+                            full + b);
+          copies = j + 3;
         }
       }
+      if (!ok) {
+        *abort_flag = 1;
+        // let the copies and MMAs already issued finish before the CTA's
+        // shared memory and TMEM go away (bounded waits)
+        for (int j = mmas; j < copies; j++) tc::mbar_wait(full + (j & 1), (uint32_t)((j >> 1) & 1));
+        if (mmas > 0) tc::mbar_wait(done + ((mmas - 1) & 1), (uint32_t)(((mmas - 1) >> 1) & 1));
+      }
     }
-    tc::fence_before_sync();
-    __syncthreads();  // accumulator b and tile b are free again
-    if (tid == 0 && j + 2 < ntiles) {
-      tc::fence_proxy_async_smem();
-      tc::mbar_arrive_expect_tx(full + b, tile_tx);
-      tc::bulk_copy_g2s(sb(b), reinterpret_cast<const unsigned char *>(rep_tiles) +
-                                   (size_t)(j + 2) * b_bytes,
-                        (uint32_t)b_bytes, full + b);
-    }
-  }
-  // merge the chains: largest value, then lowest index
-  float bv = best[0];
-  int bi = bidx[0];
+  } else {
+    const int quad = warp & 3, half = warp >> 2;
+    const int cbeg = half * (TN / 2);
+    float best[4];
+    int bidx[4];
 #pragma unroll
-  for (int c = 1; c < 4; c++)
-    if (best[c] > bv || (best[c] == bv && bidx[c] < bi)) {
-      bv = best[c];
-      bi = bidx[c];
+    for (int c = 0; c < 4; c++) {
+      best[c] = __int_as_float(0xff800000);
+      bidx[c] = 0;
     }
-  const int rrow = quad * 32 + lane;
-  if (half == 1) {
-    pv[rrow] = bv;
-    pi[rrow] = bi;
-  }
-  __syncthreads();
-  if (half == 0) {
-    const float ov = pv[rrow];
-    const int oi = pi[rrow];
-    if (ov > bv || (ov == bv && oi < bi)) {
-      bv = ov;
-      bi = oi;
+    for (int j = 0; j < ntiles; j++) {
+      const int b = j & 1;
+      // warp-uniform: tcgen05.ld needs the whole warp
+      if (!__all_sync(kFull, *abort_flag == 0 && tc::mbar_wait(done + b, (uint32_t)((j >> 1) & 1)))) {
+        *abort_flag = 1;
+        break;
+      }
+      tc::fence_after_sync();
+      const uint32_t lane_base =
+          tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * TN + cbeg);
+      const int jbase = j * TN + cbeg;
+#pragma unroll 1
+      for (int c0 = 0; c0 < TN / 2; c0 += 32) {
+        float acc[32];
+        tc::tmem_ld_32x32(lane_base + (uint32_t)c0, acc);
+#pragma unroll
+        for (int jj = 0; jj < 32; jj++) {
+          if (acc[jj] > best[jj & 3]) {
+            best[jj & 3] = acc[jj];
+            bidx[jj & 3] = jbase + c0 + jj;
+          }
+        }
+      }
+      tc::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(empty + b);
     }
-    const int64_t gr = row0 + rrow;
-    // a point whose distances are all NaN keeps index 0: a valid cluster
-    if (gr < n) cl[gr] = ok ? bi : 0;
-  }
-  if (!ok) {
-    if (tid == 0) atomicExch(err, 1);
-    // let the copies already issued land before the CTA's memory goes away
-    if (tid == 0)
-      for (int bb = 0; bb < 2; bb++) tc::mbar_wait(full + bb, 0), tc::mbar_wait(full + bb, 1);
+    // merge the chains: largest value, then lowest index
+    bv = best[0];
+    bi = bidx[0];
+#pragma unroll
+    for (int c = 1; c < 4; c++)
+      if (best[c] > bv || (best[c] == bv && bidx[c] < bi)) {
+        bv = best[c];
+        bi = bidx[c];
+      }
+    if (half == 1) {
+      pv[quad * 32 + lane] = bv;
+      pi[quad * 32 + lane] = bi;
+    }
   }
   tc::fence_before_sync();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, ncols);
+  const bool ok = *abort_flag == 0;
+  if (warp < 4) {
+    const int rrow = warp * 32 + lane;
+    const float ov = pv[rrow];
+    const int oi = pi[rrow];
+    if (ov > bv || (ov == bv && oi < bi)) bi = oi;
+    const int64_t gr = row0 + rrow;
+    // a point whose values are all NaN keeps index 0: a valid cluster
+    if (gr < n) cl[gr] = ok ? bi : 0;
+  }
+  if (!ok && tid == 0) atomicExch(err, 1);
+  if (warp == 0) {
+    __syncwarp();
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, ncols);
+  }
 }
 
 // Exact FP32 distance of every point to its chosen representative.
@@ -283,7 +317,7 @@ int launch_assign_tc(const float4 *rows, int64_t n, int dp4, int d, const float4
   // (measured faster than 256-row tiles with one CTA per SM)
   const int TN = kTileN / 2;
   const size_t need = tc::tile_bytes(kTileM, KD) + 2 * tc::tile_bytes(TN, KD) +
-                      4 * sizeof(uint64_t) + 16 + (size_t)kTileM * 8;
+                      6 * sizeof(uint64_t) + 16 + (size_t)kTileM * 8;
   // a CTA holds 2 x TN TMEM columns: with TN = 256 that is all 512, so at
   // most one CTA per SM (over 114 KB each), with TN = 128 at most two
   const size_t smem = std::max<size_t>(need, TN == kTileN ? 116 * 1024 : 80 * 1024);
@@ -293,7 +327,7 @@ int launch_assign_tc(const float4 *rows, int64_t n, int dp4, int d, const float4
                                     cudaFuncAttributePreferredSharedMemoryCarveout,
                                     cudaSharedmemCarveoutMaxShared));
   const int64_t blocks = (n + kTileM - 1) / kTileM;
-  assign_tc_kernel<<<(unsigned)blocks, 256, smem, s>>>(rows, n, dp4, d, KD, TN, tiles,
+  assign_tc_kernel<<<(unsigned)blocks, kAssignThreads, smem, s>>>(rows, n, dp4, d, KD, TN, tiles,
                                                        Rpad / TN, cl, err);
   KNN_LAUNCH_CHECK();
   exact_rep_dist_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 32), 256, 0, s>>>(

@@ -105,6 +105,11 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *mbar, uint32_t b
                :: "r"(smem_u32(mbar)), "r"(bytes) : "memory");
 }
 
+// One plain arrival on the mbarrier.
+__device__ __forceinline__ void mbar_arrive(uint64_t *mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(mbar)) : "memory");
+}
+
 // 1-D bulk asynchronous copy global -> this CTA's shared memory (no
 // multicast), completing `bytes` of transaction count on the mbarrier.  Both
 // addresses 16-byte aligned, bytes a multiple of 16.
