@@ -98,7 +98,9 @@ __global__ void reps_to_bf16_tiles_kernel(const float4 *__restrict__ reps, int R
 // the other warps check before their next wait.
 // dynamic shared memory: A tile, 2 B tiles, 6 mbarriers, TMEM slot, abort
 // flag, 128 (value, index) pairs
-constexpr int kAssignThreads = 288;
+// epilogue warps split the TN columns kEsplit ways (4 measured no faster)
+constexpr int kEsplit = 2;
+constexpr int kAssignThreads = 128 * kEsplit + 32;
 
 __global__ void __launch_bounds__(kAssignThreads, 1)
     assign_tc_kernel(const float4 *__restrict__ rows, int64_t n, int dp4, int d, int KD, int TN,
@@ -114,8 +116,8 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
   uint64_t *empty = done + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(empty + 2);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
-  float *pv = reinterpret_cast<float *>(tmem_slot + 4);  // 128 partial maxima
-  int *pi = reinterpret_cast<int *>(pv + kTileM);
+  float *pv = reinterpret_cast<float *>(tmem_slot + 4);  // kEsplit x 128 partial maxima
+  int *pi = reinterpret_cast<int *>(pv + kEsplit * kTileM);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t row0 = (int64_t)blockIdx.x * kTileM;
@@ -127,13 +129,13 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
     for (int i = 0; i < 2; i++) {
       tc::mbar_init(full + i, 1);
       tc::mbar_init(done + i, 1);
-      tc::mbar_init(empty + i, 8);
+      tc::mbar_init(empty + i, 4 * kEsplit);
     }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  const bool producer = warp == 8 && lane == 0;
+  const bool producer = warp == 4 * kEsplit && lane == 0;
   // first two representative tiles in flight while the points are staged
   if (producer)
     for (int j = 0; j < 2 && j < ntiles; j++) {
@@ -168,7 +170,7 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
 
   float bv = __int_as_float(0xff800000);
   int bi = 0;
-  if (warp == 8) {
+  if (warp == 4 * kEsplit) {
     if (producer) {
       const uint32_t idesc = tc::make_idesc_bf16(kTileM, TN);
       const uint32_t a_base = tc::smem_u32(sa);
@@ -215,8 +217,8 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
       }
     }
   } else {
-    const int quad = warp & 3, half = warp >> 2;
-    const int cbeg = half * (TN / 2);
+    const int quad = warp & 3, part = warp >> 2;
+    const int cbeg = part * (TN / kEsplit);
     float best[4];
     int bidx[4];
 #pragma unroll
@@ -236,7 +238,7 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
           tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(b * TN + cbeg);
       const int jbase = j * TN + cbeg;
 #pragma unroll 1
-      for (int c0 = 0; c0 < TN / 2; c0 += 32) {
+      for (int c0 = 0; c0 < TN / kEsplit; c0 += 32) {
         float acc[32];
         tc::tmem_ld_32x32(lane_base + (uint32_t)c0, acc);
 #pragma unroll
@@ -260,19 +262,19 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
         bv = best[c];
         bi = bidx[c];
       }
-    if (half == 1) {
-      pv[quad * 32 + lane] = bv;
-      pi[quad * 32 + lane] = bi;
-    }
+    pv[part * kTileM + quad * 32 + lane] = bv;
+    pi[part * kTileM + quad * 32 + lane] = bi;
   }
   tc::fence_before_sync();
   __syncthreads();
   const bool ok = *abort_flag == 0;
   if (warp < 4) {
     const int rrow = warp * 32 + lane;
-    const float ov = pv[rrow];
-    const int oi = pi[rrow];
-    if (ov > bv || (ov == bv && oi < bi)) bi = oi;
+    for (int q = 1; q < kEsplit; q++) {
+      const float ov = pv[q * kTileM + rrow];
+      const int oi = pi[q * kTileM + rrow];
+      if (ov > bv || (ov == bv && oi < bi)) bv = ov, bi = oi;
+    }
     const int64_t gr = row0 + rrow;
     // a point whose values are all NaN keeps index 0: a valid cluster
     if (gr < n) cl[gr] = ok ? bi : 0;
@@ -313,11 +315,11 @@ int launch_assign_tc(const float4 *rows, int64_t n, int dp4, int d, const float4
   reps_to_bf16_tiles_kernel<<<(Rpad + 127) / 128, 128, 0, s>>>(reps, R, dp4, d, KD, Rpad, tiles);
   KNN_LAUNCH_CHECK();
   // representative tiles of 128 rows: a CTA then holds 256 TMEM columns and
-  // two CTAs share an SM, whose warps hide each other's epilogue latency
-  // (measured faster than 256-row tiles with one CTA per SM)
+  // two CTAs share an SM (measured faster than 256-row tiles with one CTA
+  // per SM, with either 8 or 16 epilogue warps)
   const int TN = kTileN / 2;
   const size_t need = tc::tile_bytes(kTileM, KD) + 2 * tc::tile_bytes(TN, KD) +
-                      6 * sizeof(uint64_t) + 16 + (size_t)kTileM * 8;
+                      6 * sizeof(uint64_t) + 16 + (size_t)kEsplit * kTileM * 8;
   // a CTA holds 2 x TN TMEM columns: with TN = 256 that is all 512, so at
   // most one CTA per SM (over 114 KB each), with TN = 128 at most two
   const size_t smem = std::max<size_t>(need, TN == kTileN ? 116 * 1024 : 80 * 1024);

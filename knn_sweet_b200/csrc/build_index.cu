@@ -50,8 +50,10 @@ __global__ void pack_rows_kernel(const float *__restrict__ src, int64_t n,
 // staged through shared memory 32 floats at a time and every thread
 // accumulates TB x TB pairs (i = i0 + ty + 16a, j = j0 + tx + 16b), each
 // summed in dimension order with fma, exactly as the one-pair distance would
-// be.
-// grid: (ceil(R / 16TB), ceil(R / 16TB), trials), 256 threads
+// be.  The pair distance is symmetric bit for bit (fsub(a, b) = -fsub(b, a)
+// and squaring drops the sign), so only the tiles on and above the diagonal
+// run, and an off-diagonal tile counts twice (wrapping, like the sum).
+// grid: (nb (nb + 1) / 2 tiles, 1, trials), nb = ceil(R / 16TB), 256 threads
 // ---------------------------------------------------------------------------
 template <int TB>
 __global__ void __launch_bounds__(256)
@@ -63,7 +65,13 @@ __global__ void __launch_bounds__(256)
   __shared__ float4 sb[8][T];
   __shared__ uint32_t red[8];
   const int t = blockIdx.z;
-  const int i0 = blockIdx.x * T, j0 = blockIdx.y * T;
+  // triangle index -> tile (bi, bj), bi <= bj
+  const int tri = blockIdx.x;
+  int bj = (int)((sqrtf(8.0f * (float)tri + 1.0f) - 1.0f) * 0.5f);
+  while ((bj + 1) * (bj + 2) / 2 <= tri) bj++;
+  while (bj * (bj + 1) / 2 > tri) bj--;
+  const int bi = tri - bj * (bj + 1) / 2;
+  const int i0 = bi * T, j0 = bj * T;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int32_t *c = cand + (int64_t)t * R;
   float acc[TB][TB];
@@ -114,7 +122,7 @@ __global__ void __launch_bounds__(256)
   if (threadIdx.x == 0) {
     uint32_t tot = 0;
     for (int w = 0; w < 8; w++) tot += red[w];
-    atomicAdd(score + t, tot);
+    atomicAdd(score + t, bi == bj ? tot : 2u * tot);
   }
 }
 
@@ -553,7 +561,8 @@ int launch_rep_select(const float4 *rows, int dp4, const int32_t *cand_dev,
   KNN_CUDA_TRY(cudaMemsetAsync(score_dev, 0, sizeof(uint32_t) * trials, s));
   // 4 x 4 pairs per thread: 8 x 8 (fewer shared-memory loads per fma) took
   // about 160 registers and measured slower on 8,192 representatives
-  dim3 grid((R + 63) / 64, (R + 63) / 64, trials);
+  const int nb = (R + 63) / 64;
+  dim3 grid((unsigned)(nb * (nb + 1) / 2), 1, trials);
   rep_score_kernel<4><<<grid, 256, 0, s>>>(rows, dp4, cand_dev, R, score_dev);
   KNN_LAUNCH_CHECK();
   rep_pick_kernel<<<1, 256, 0, s>>>(rows, dp4, cand_dev, R, trials, score_dev,
