@@ -20,7 +20,8 @@ namespace knnsweet {
 //  2. The reference clusters Rs that can hold a point within theta0 of some
 //     query of the cluster: d(Rq,Rs) - rq - radius(Rs) <= theta0
 //     (FilterReps, knnjoin.cu:506-525), sorted by d(Rq,Rs), then Rs
-//     (the host std::sort of knnjoin.cu:1080-1091).
+//     (the host std::sort of knnjoin.cu:1080-1091); only the survivors
+//     enter the sort.
 // ---------------------------------------------------------------------------
 // One query cluster's bound and candidate list, by one block.  The reference
 // clusters are the Rs_loc consecutive clusters whose offsets start at soff
@@ -122,23 +123,24 @@ static __device__ __forceinline__ void bounds_filter_block(const float *dq, int 
   }
   __syncthreads();
 
-  // filter + sort the survivors by (d(Rq,Rs), Rs)
-  for (int j = tid; j < rs_pow2; j += nth) {
-    uint64_t key = kKeyMax;
-    if (j < Rs_loc && soff[j + 1] > soff[j]) {
+  // filter: the survivors are compacted into skey (in any order; the keys
+  // are distinct), then only those are sorted by (d(Rq,Rs), Rs)
+  for (int j = tid; j < Rs_loc; j += nth) {
+    if (soff[j + 1] > soff[j]) {
       float dd = dq[j], rr = scmax[j];
       float lb = dd - rq - rr;
-      if (!(lb > th + tol * (dd + rq + rr + th))) {
-        key = ((uint64_t)__float_as_uint(dd) << 32) | (uint32_t)j;
-        atomicAdd(&kept_s, 1);
-      }
+      if (!(lb > th + tol * (dd + rq + rr + th)))
+        skey[atomicAdd(&kept_s, 1)] = ((uint64_t)__float_as_uint(dd) << 32) | (uint32_t)j;
     }
-    skey[j] = key;
   }
   __syncthreads();
-  for (int size = 2; size <= rs_pow2; size <<= 1) {
+  int p2 = 1;  // <= rs_pow2: a power of two >= Rs_loc >= kept
+  while (p2 < kept_s) p2 <<= 1;
+  for (int j = kept_s + tid; j < p2; j += nth) skey[j] = kKeyMax;
+  __syncthreads();
+  for (int size = 2; size <= p2; size <<= 1) {
     for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int t = tid; t < (rs_pow2 >> 1); t += nth) {
+      for (int t = tid; t < (p2 >> 1); t += nth) {
         int i = 2 * t - (t & (stride - 1));
         int j = i + stride;
         bool up = (i & size) == 0;
