@@ -36,7 +36,7 @@ static __device__ __forceinline__ void bounds_filter_block(const float *dq, int 
                                     float *theta0_out, int32_t *rlist_out,
                                     int32_t *rlen_out) {
   __shared__ int red_i[32];
-  __shared__ unsigned red_u[32];
+  __shared__ unsigned red_u[32], red_l[32];
   __shared__ int kept_s;
   const int tid = threadIdx.x, nth = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarp = nth >> 5;
@@ -58,7 +58,7 @@ static __device__ __forceinline__ void bounds_filter_block(const float *dq, int 
   // below): a cluster whose smallest value exceeds T adds nothing to the
   // count at T and skips its search.
   float *lo_v = reinterpret_cast<float *>(skey);
-  unsigned hi_local = 0, u_local = 0xffffffffu;
+  unsigned hi_local = 0, u_local = 0xffffffffu, l_local = 0xffffffffu;
   for (int j = tid; j < Rs_loc; j += nth) {
     int a = soff[j], sz = min(soff[j + 1] - a, kk);
     float first = __int_as_float(0x7f800000);
@@ -68,27 +68,31 @@ static __device__ __forceinline__ void bounds_filter_block(const float *dq, int 
       hi_local = max(hi_local, __float_as_uint(v));
       if (sz == kk) u_local = min(u_local, __float_as_uint(v));
       first = __fadd_rn(base, sdist[a]);
+      l_local = min(l_local, __float_as_uint(first));
     }
     lo_v[j] = first;
   }
   for (int o = 16; o > 0; o >>= 1) {
     hi_local = max(hi_local, __shfl_xor_sync(kFull, hi_local, o));
     u_local = min(u_local, __shfl_xor_sync(kFull, u_local, o));
+    l_local = min(l_local, __shfl_xor_sync(kFull, l_local, o));
   }
   if (lane == 0) {
     red_u[warp] = hi_local;
     red_i[warp] = (int)u_local;
+    red_l[warp] = l_local;
   }
   __syncthreads();
-  unsigned hi = 0, u = 0xffffffffu;
+  unsigned hi = 0, u = 0xffffffffu, lo = 0xffffffffu;
   for (int w = 0; w < nwarp; w++) {
     hi = max(hi, red_u[w]);
     u = min(u, (unsigned)red_i[w]);
+    lo = min(lo, red_l[w]);
   }
   if (u < hi) hi = u;
   __syncthreads();
   // smallest bit pattern T with count(values <= T) >= kk; count(hi) >= kk.
-  unsigned lo = 0;  // count(lo - 1) < kk is implied for lo = 0
+  // lo: the smallest value of all (nothing lies below it), lo <= hi
   // invariant: answer in [lo, hi]
   while (lo < hi) {
     unsigned mid = lo + ((hi - lo) >> 1);
