@@ -73,6 +73,8 @@ struct RegTopK : TopKBase {
   }
 
   __device__ __forceinline__ void make_room(int lane) { flush(lane); }
+  // end of the query: pending candidates merged into the list
+  __device__ __forceinline__ void finish(int lane) { flush(lane); }
 
   __device__ __forceinline__ void flush(int lane) {
     if (nbuf == 0) return;
@@ -193,6 +195,8 @@ struct SmemTopK : TopKBase {
   }
 
   __device__ __forceinline__ void make_room(int lane) { flush(lane); }
+  // end of the query: pending candidates merged into the list
+  __device__ __forceinline__ void finish(int lane) { flush(lane); }
 
   __device__ __forceinline__ void flush(int lane) {
     if (nbuf == 0) return;
@@ -302,6 +306,11 @@ struct SelectTopK : TopKBase {
     thr = ((uint64_t)T << 32) | 0xffffffffull;
     theta = sqrtf(__uint_as_float(T));
   }
+
+  // End of the query: nothing to do -- write_out sorts up to L keys as they
+  // are (their first k are the answer) and selects the exact k-th key first
+  // only beyond that, which saves the 64-bit selection for most queries.
+  __device__ __forceinline__ void finish(int) {}
 
   __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int32_t base, int lane) {
     // up to L keys are sorted as they are (their first k are the answer);
@@ -569,6 +578,8 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, L, WARPS>())
       // visit this chunk's surviving clusters: in list order (by rep-rep
       // distance) or, with KNN_ORDER_BY_D, nearest d(q, Rs) first
       unsigned amask = __ballot_sync(kFull, alive);
+      if (amask == 0) continue;  // warp-uniform: nothing to visit in this batch
+      const int nalive = __popc(amask);
       float dkey = alive ? D : __int_as_float(0x7f800000);
       // Visit order: nearest d(q, Rs) first.  Narrow rows sort the batch once
       // (bitonic network over the 32 lanes, ties to the lower lane: less work
@@ -577,7 +588,7 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, L, WARPS>())
       constexpr bool kSortBatch = KNN_ORDER_BY_D != 0 && DP4 >= 1 && DP4 <= 2;
       float sv = dkey;
       int sl = lane;
-      if constexpr (kSortBatch) {
+      if (kSortBatch && nalive > 1) {  // a single survivor needs no order
 #pragma unroll
         for (int size = 2; size <= 32; size <<= 1) {
 #pragma unroll
@@ -593,11 +604,10 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, L, WARPS>())
           }
         }
       }
-      const int nalive = __popc(amask);
       for (int rank = 0; rank < nalive; rank++) {
         int src;
         if constexpr (kSortBatch) {
-          src = __shfl_sync(kFull, sl, rank);
+          src = nalive > 1 ? __shfl_sync(kFull, sl, rank) : __ffs(amask) - 1;
         } else {
           src = __ffs(amask) - 1;
 #if KNN_ORDER_BY_D
@@ -678,7 +688,7 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, L, WARPS>())
 #endif
       }
     }
-    tk.flush(lane);
+    tk.finish(lane);
     tk.write_out(a.out_idx + q * a.k, a.out_dist + q * a.k, a.squared,
                  a.qc_ref_base ? (int32_t)a.qc_ref_base[qc] : 0, lane);
     if (a.counters) {
