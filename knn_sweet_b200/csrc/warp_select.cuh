@@ -99,21 +99,42 @@ __device__ __forceinline__ uint64_t warp_select_kth(const uint64_t *s, int n, in
 
 // k-th smallest (1-based, 1 <= k <= n) of the 32-bit values s[i * stride],
 // i < n, which may repeat: the value v with #{s < v} < k <= #{s <= v}.  One
-// warp, four 8-bit digit passes over s (global or shared memory); `hist` is
-// a 256-word shared-memory histogram.  Non-negative floats order like their
+// warp, 8-bit digit passes over s (global or shared memory) restricted to the
+// bits that differ between the values -- an OR / AND pass finds them; on
+// small integers stored as floats (squared distances of integer points) the
+// low mantissa bits are all zero and two passes replace four.  `hist` is a
+// 256-word shared-memory histogram.  Non-negative floats order like their
 // bit patterns, so this also selects among non-negative floats.
 __device__ __forceinline__ uint32_t warp_select_kth_u32(const uint32_t *s, int stride, int n,
                                                         int k, uint32_t *hist, int lane) {
-  uint32_t prefix = 0, known = 0, need = (uint32_t)k;
+  uint32_t vor = 0u, vand = 0xffffffffu;
+  for (int i = lane; i < n; i += 32) {
+    const uint32_t v = s[(size_t)i * stride];
+    vor |= v;
+    vand &= v;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    vor |= __shfl_xor_sync(kFull, vor, o);
+    vand &= __shfl_xor_sync(kFull, vand, o);
+  }
+  const uint32_t diff = vor ^ vand;  // bits in which some values differ
+  if (diff == 0u) return vand;       // all equal
+  const int hb = 31 - __clz(diff), lb = __ffs(diff) - 1;
+  // bits above hb and below lb are the same in every value
+  uint32_t known = hb == 31 ? 0u : (0xffffffffu << (hb + 1));
+  uint32_t prefix = vand & known, need = (uint32_t)k;
 #pragma unroll 1
-  for (int shift = 24; shift >= 0; shift -= 8) {
+  for (int top = hb + 1; top > lb;) {
+    const int shift = top - 8 > lb ? top - 8 : lb;
+    const uint32_t dmask = (1u << (top - shift)) - 1u;
     __syncwarp();
 #pragma unroll
     for (int b = 0; b < 8; b++) hist[b * 32 + lane] = 0;
     __syncwarp();
     for (int i = lane; i < n; i += 32) {
       const uint32_t v = s[(size_t)i * stride];
-      if ((v & known) == prefix) atomicAdd(&hist[(v >> shift) & 255u], 1u);
+      if ((v & known) == prefix) atomicAdd(&hist[(v >> shift) & dmask], 1u);
     }
     __syncwarp();
     uint32_t base = 0, before = 0;
@@ -137,10 +158,11 @@ __device__ __forceinline__ uint32_t warp_select_kth_u32(const uint32_t *s, int s
     }
     need -= before;
     prefix |= (uint32_t)bin << shift;
-    known |= 255u << shift;
+    known |= dmask << shift;
+    top = shift;
   }
   __syncwarp();
-  return prefix;
+  return prefix | (vand & ((1u << lb) - 1u));  // the common low bits
 }
 
 // ---------------------------------------------------------------------------
