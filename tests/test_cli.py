@@ -71,6 +71,63 @@ def test_text_reader_crlf_and_token_stream(tmp_path):
     assert np.array_equal(r.reshape(-1), stream[:300])
 
 
+def _float_text(vals, rng):
+    """float32 values as text in mixed spellings and separators."""
+    seps = [" ", "\t", "\n", "\r\n", "  \t "]
+    parts = []
+    for i, v in enumerate(vals):
+        form = ("%.9g", "%.8e", "%.9G")[i % 3]
+        parts.append(form % float(v))
+        parts.append(seps[rng.integers(len(seps))])
+    return "".join(parts)
+
+
+def test_parallel_text_reader_equals_serial_reading(tmp_path):
+    rng = np.random.default_rng(11)
+    vals = (rng.standard_normal(120_000) * 10.0 ** rng.integers(-6, 7, 120_000)).astype(np.float32)
+    f = tmp_path / "big.txt"
+    f.write_text(_float_text(vals, rng))
+    assert f.stat().st_size > 16 * (1 << 16)  # many chunks
+    out = tmp_path / "in.bin"
+    run_cli([40_000, 30_000, 3, 8, 8, 5, f, f],
+            {"KNNJOIN_DUMP_INPUT": str(out), "OMP_NUM_THREADS": "4"})
+    q, r = dumped_inputs(out, 40_000, 30_000, 3)
+    assert np.array_equal(q.reshape(-1), vals) and np.array_equal(r.reshape(-1), vals[:90_000])
+
+
+def test_parallel_text_reader_stops_like_fscanf(tmp_path):
+    """Text that is not a whole number deep in the file: "1.5-2" reads as two
+    values, "7abc" as 7 followed by the end of the input, as successive
+    fscanf("%f") calls read them; the slots past the end stay zero."""
+    rng = np.random.default_rng(12)
+    a = rng.standard_normal(60_000).astype(np.float32)
+    b = rng.standard_normal(30_000).astype(np.float32)
+    c = rng.standard_normal(20_000).astype(np.float32)
+    f = tmp_path / "odd.txt"
+    f.write_text(_float_text(a, rng) + " 1.5-2 " + _float_text(b, rng) + " 7abc "
+                 + _float_text(c, rng))
+    want = np.concatenate([a, [1.5, -2.0], b, [7.0]]).astype(np.float32)
+    m = want.size + 50
+    out = tmp_path / "in.bin"
+    res = run_cli([m, 1000, 1, 8, 8, 5, f, f],
+                  {"KNNJOIN_DUMP_INPUT": str(out), "OMP_NUM_THREADS": "4"})
+    assert "error reading" in res.stdout
+    q, r = dumped_inputs(out, m, 1000, 1)
+    assert np.array_equal(q[:want.size, 0], want) and not q[want.size:].any()
+    assert np.array_equal(r[:, 0], a[:1000])
+
+
+def test_raw_float32_inputs(tmp_path):
+    rng = np.random.default_rng(13)
+    x = rng.standard_normal((500, 4)).astype(np.float32)
+    f = tmp_path / "pts.f32"
+    x.tofile(f)
+    out = tmp_path / "in.bin"
+    run_cli([500, 300, 4, 8, 8, 5, f, f], {"KNNJOIN_DUMP_INPUT": str(out)})
+    q, r = dumped_inputs(out, 500, 300, 4)
+    assert np.array_equal(q, x) and np.array_equal(r, x[:300])
+
+
 def test_missing_file_is_an_error(tmp_path):
     res = run_cli([5, 5, 3, 2, 2, 2, tmp_path / "nope.txt", tmp_path / "nope.txt"], check=False)
     assert res.returncode == 1 and "error opening" in res.stdout
