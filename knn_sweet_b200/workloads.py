@@ -1,6 +1,6 @@
 """Run one join of a named benchmark configuration and print its statistics.
 
-    python -m knn_sweet_b200.workloads c1|c2|c3|c3-small|c4|c5 [--form fp32|bf16_refine]
+    python -m knn_sweet_b200.workloads c1|c2|c3|c3-small|c4|c4-small|c5 [--form fp32|bf16_refine]
                                        [--repeat N]
 
   c1        skin-like self-join, N = M = 245,057, d = 3, k = 200, reps 800/800
@@ -9,6 +9,7 @@
   c3-small  N = 400,000, M = 40,000, d = 128, k = 100, reps 1600/1600, 4 steps (sized
             for profiler captures: inputs above L2, a few hundred MB on the device)
   c4        4,096 ellipsoid clouds (256..16,384 points), d = 3, per-cloud self-join, k = 16
+  c4-small  512 clouds of the same sizes, no autotuning (sized for profiler captures)
   c5        64 blob cloud pairs (2,048..32,768 points), d = 3, k = 8 in both directions,
             forward + backward of the summed loss
 
@@ -41,7 +42,7 @@ def _pair_join(name, q, r, k, form, repeat, **kw):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("workload", choices=["c1", "c2", "c3", "c3-small", "c4", "c5"])
+    ap.add_argument("workload", choices=["c1", "c2", "c3", "c3-small", "c4", "c4-small", "c5"])
     ap.add_argument("--form", choices=["fp32", "bf16_refine"], default="fp32")
     ap.add_argument("--repeat", type=int, default=1)
     a = ap.parse_args(argv)
@@ -59,14 +60,16 @@ def main(argv=None):
                                  sigma=0.5)
         _pair_join("c3-small", q, r, 100, a.form, a.repeat, qreps=1600, sreps=1600,
                    lloyd_iters=4)
-    elif a.workload == "c4":
+    elif a.workload in ("c4", "c4-small"):
         from .batched import knnjoin_batched
-        pts, off = data.ellipsoid_clouds()
+        small = a.workload == "c4-small"
+        pts, off = data.ellipsoid_clouds(nclouds=512 if small else 4096)
         x = torch.from_numpy(pts).cuda()
         for _ in range(a.repeat):
-            _, _, st = knnjoin_batched(x, off, k=16, stats=True)
-        print(f"c4 clouds={len(off) - 1} points={x.shape[0]}: total {st.ms_total:.2f} ms "
-              f"(build {st.ms_build:.2f}, search {st.ms_search:.2f})", flush=True)
+            _, _, st = knnjoin_batched(x, off, k=16, autotune=not small, stats=True)
+        print(f"{a.workload} clouds={len(off) - 1} points={x.shape[0]}: total "
+              f"{st.ms_total:.2f} ms (build {st.ms_build:.2f}, search {st.ms_search:.2f})",
+              flush=True)
     else:
         from .autograd import knn_chamfer_batched
         pairs = data.blob_cloud_pairs()
