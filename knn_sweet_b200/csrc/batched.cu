@@ -201,6 +201,50 @@ __global__ void __launch_bounds__(512)
                       skey, theta0 + qc, rlist + base, rlen + qc);
 }
 
+// The same per query cluster, one warp each (clouds with at most a few
+// hundred representatives): kBoundsWarps warps per block, each with its own
+// `per_warp` bytes of dynamic shared memory (rs_pow2 keys, then max_rs floats).
+constexpr int kBoundsWarps = 8;
+
+__global__ void __launch_bounds__(kBoundsWarps * 32)
+    batched_bounds_warp_kernel(const float4 *__restrict__ qreps, const float4 *__restrict__ sreps,
+                               int dp4, const int32_t *__restrict__ q_roff,
+                               const int32_t *__restrict__ s_roff,
+                               const int64_t *__restrict__ pair_off,
+                               const int64_t *__restrict__ r_poff, int ncloud, int nqc,
+                               const int32_t *__restrict__ qoff, const int32_t *__restrict__ soff,
+                               const float *__restrict__ sdist, const float *__restrict__ scmax,
+                               const float *__restrict__ qrad, int k, int d, int rs_pow2,
+                               int per_warp, float *__restrict__ theta0,
+                               int32_t *__restrict__ rlist, int32_t *__restrict__ rlen,
+                               int64_t *__restrict__ rl_base, int64_t *__restrict__ qc_ref_base) {
+  extern __shared__ __align__(16) unsigned char wsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int qc = blockIdx.x * kBoundsWarps + warp;
+  if (qc >= nqc) return;  // whole warps only; no block barrier follows
+  uint64_t *skey = reinterpret_cast<uint64_t *>(wsm + (size_t)warp * per_warp);
+  float *dq = reinterpret_cast<float *>(skey + rs_pow2);
+  const int c = cloud_of(q_roff, ncloud, qc);
+  const int sb = s_roff[c], Rs_loc = s_roff[c + 1] - sb;
+  const int64_t base = pair_off[c] + (int64_t)(qc - q_roff[c]) * Rs_loc;
+  if (lane == 0) {
+    rl_base[qc] = base;
+    qc_ref_base[qc] = r_poff[c];
+  }
+  if (qoff[qc + 1] == qoff[qc] || Rs_loc == 0) {
+    if (lane == 0) {
+      theta0[qc] = 0.0f;
+      rlen[qc] = 0;
+    }
+    return;
+  }
+  for (int j = lane; j < Rs_loc; j += 32)
+    dq[j] = sqrtf(dist2_rows_rt(qreps + (int64_t)qc * dp4, sreps + (int64_t)(sb + j) * dp4, dp4));
+  __syncwarp();
+  bounds_filter_warp(dq, Rs_loc, soff + sb, sdist, scmax + sb, qrad[qc], k, d, sb, skey,
+                     theta0 + qc, rlist + base, rlen + qc, lane);
+}
+
 __global__ void batched_fill_empty_kernel(int32_t *idx, float *dist, int64_t count) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
        t += (int64_t)gridDim.x * blockDim.x) {
@@ -447,15 +491,32 @@ int batched_impl(const float *q, const int64_t *qoff_h, const float *r, const in
         int p2 = 1;
         while (p2 < S.maxR) p2 <<= 1;
         const size_t smem = (size_t)p2 * sizeof(uint64_t) + (size_t)S.maxR * sizeof(float);
-        if (smem > 48 * 1024)
-          KNN_CUDA_TRY(cudaFuncSetAttribute(batched_bounds_kernel,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)smem));
-        const int nth = std::min(512, std::max(64, p2 / 2));
-        batched_bounds_kernel<<<Q.Rtot, nth, smem, s>>>(
-            Q.reps, S.reps, dp4, Q.roff, S.roff, pair_off, S.poff, ncloud, Q.off, S.off, sdist,
-            cmax, qrad, k, d, p2, theta0, rlist, rlen, rl_base, qc_ref_base);
-        KNN_LAUNCH_CHECK();
+        // a warp per query cluster while each warp's share of shared memory
+        // is small (up to 512 representatives per cloud); a block otherwise
+        const int per_warp = (int)((smem + 15) & ~(size_t)15);
+        if (per_warp <= 6 * 1024) {
+          const size_t wsmem = (size_t)kBoundsWarps * per_warp;
+          if (wsmem > 48 * 1024)
+            KNN_CUDA_TRY(cudaFuncSetAttribute(batched_bounds_warp_kernel,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)wsmem));
+          batched_bounds_warp_kernel<<<(unsigned)((Q.Rtot + kBoundsWarps - 1) / kBoundsWarps),
+                                       kBoundsWarps * 32, wsmem, s>>>(
+              Q.reps, S.reps, dp4, Q.roff, S.roff, pair_off, S.poff, ncloud, (int)Q.Rtot, Q.off,
+              S.off, sdist, cmax, qrad, k, d, p2, per_warp, theta0, rlist, rlen, rl_base,
+              qc_ref_base);
+          KNN_LAUNCH_CHECK();
+        } else {
+          if (smem > 48 * 1024)
+            KNN_CUDA_TRY(cudaFuncSetAttribute(batched_bounds_kernel,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem));
+          const int nth = std::min(512, std::max(64, p2 / 2));
+          batched_bounds_kernel<<<Q.Rtot, nth, smem, s>>>(
+              Q.reps, S.reps, dp4, Q.roff, S.roff, pair_off, S.poff, ncloud, Q.off, S.off,
+              sdist, cmax, qrad, k, d, p2, theta0, rlist, rlen, rl_base, qc_ref_base);
+          KNN_LAUNCH_CHECK();
+        }
       }
       if (st) KNN_CUDA_TRY(cudaEventRecord(ev[1], s));
       ScanArgs a{};

@@ -4,6 +4,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "warp_select.cuh"
 
 namespace knnsweet {
 
@@ -161,6 +162,99 @@ static __device__ __forceinline__ void bounds_filter_block(const float *dq, int 
   for (int j = tid; j < kept; j += nth)
     rlist_out[j] = id_base + (int32_t)(skey[j] & 0xffffffffu);
   if (tid == 0) *rlen_out = kept;
+}
+
+// The same bound and candidate list by one warp, for query clusters with few
+// reference clusters (the batched form: one cloud's representatives, a few
+// hundred at most).  Identical arithmetic -- the bisection counts, the filter
+// test and the sort keys are the block version's -- with shuffle reductions
+// instead of block barriers and a ballot compaction of the survivors (the
+// sort makes their order the same).  skey: rs_pow2 >= Rs_loc keys of this
+// warp's shared memory.
+static __device__ __forceinline__ void bounds_filter_warp(
+    const float *dq, int Rs_loc, const int32_t *__restrict__ soff,
+    const float *__restrict__ sdist, const float *__restrict__ scmax, float rq, int k, int d,
+    int32_t id_base, uint64_t *skey, float *theta0_out, int32_t *rlist_out,
+    int32_t *rlen_out, int lane) {
+  const float tol = bound_tol(d);
+  const int64_t n = soff[Rs_loc] - soff[0];
+  const int kk = (int)(k < n ? k : n);
+  if (kk == 0) {
+    if (lane == 0) {
+      *theta0_out = 0.0f;
+      *rlen_out = 0;
+    }
+    return;
+  }
+  float *lo_v = reinterpret_cast<float *>(skey);
+  unsigned hi = 0, u = 0xffffffffu, lo = 0xffffffffu;
+  for (int j = lane; j < Rs_loc; j += 32) {
+    const int a = soff[j], sz = min(soff[j + 1] - a, kk);
+    float first = __int_as_float(0x7f800000);
+    if (sz > 0) {
+      const float base = __fadd_rn(rq, dq[j]);
+      const float v = __fadd_rn(base, sdist[a + sz - 1]);
+      hi = max(hi, __float_as_uint(v));
+      if (sz == kk) u = min(u, __float_as_uint(v));
+      first = __fadd_rn(base, sdist[a]);
+      lo = min(lo, __float_as_uint(first));
+    }
+    lo_v[j] = first;
+  }
+  hi = __reduce_max_sync(kFull, hi);
+  u = __reduce_min_sync(kFull, u);
+  lo = __reduce_min_sync(kFull, lo);
+  if (u < hi) hi = u;
+  __syncwarp();
+  // smallest bit pattern T with count(values <= T) >= kk, in [lo, hi]
+  while (lo < hi) {
+    const unsigned mid = lo + ((hi - lo) >> 1);
+    const float T = __uint_as_float(mid);
+    int cnt = 0;
+    for (int j = lane; j < Rs_loc; j += 32) {
+      if (lo_v[j] > T) continue;
+      const int a = soff[j], sz = min(soff[j + 1] - a, kk);
+      const float base = __fadd_rn(rq, dq[j]);
+      int l = 0, h = sz;
+      while (l < h) {
+        const int md = (l + h) >> 1;
+        if (__fadd_rn(base, sdist[a + md]) <= T) l = md + 1;
+        else h = md;
+      }
+      cnt += l;
+    }
+    if ((int)__reduce_add_sync(kFull, (unsigned)cnt) >= kk) hi = mid;
+    else lo = mid + 1;
+  }
+  const float kth = __uint_as_float(hi);
+  const float th = __fmaf_rn(kth, 4.0f * tol, kth) + 1.17549435e-38f;
+  __syncwarp();
+  // survivors compacted in cluster order, then sorted by (d(Rq,Rs), Rs)
+  int kept = 0;
+  for (int j0 = 0; j0 < Rs_loc; j0 += 32) {
+    const int j = j0 + lane;
+    bool keep = false;
+    uint64_t key = 0;
+    if (j < Rs_loc && soff[j + 1] > soff[j]) {
+      const float dd = dq[j], rr = scmax[j];
+      const float lb = dd - rq - rr;
+      keep = !(lb > th + tol * (dd + rq + rr + th));
+      key = ((uint64_t)__float_as_uint(dd) << 32) | (uint32_t)j;
+    }
+    const unsigned bm = __ballot_sync(kFull, keep);
+    if (keep) skey[kept + __popc(bm & ((1u << lane) - 1u))] = key;
+    kept += __popc(bm);
+  }
+  int p2 = 1;
+  while (p2 < kept) p2 <<= 1;
+  for (int j = kept + lane; j < p2; j += 32) skey[j] = kKeyMax;
+  __syncwarp();
+  smem_bitonic_sort_rt(skey, p2, lane);
+  for (int j = lane; j < kept; j += 32) rlist_out[j] = id_base + (int32_t)(skey[j] & 0xffffffffu);
+  if (lane == 0) {
+    *theta0_out = th;
+    *rlen_out = kept;
+  }
 }
 
 }  // namespace knnsweet
