@@ -89,10 +89,19 @@ __global__ void __launch_bounds__(256)
   for (int e = threadIdx.x; e < R * dp4; e += blockDim.x)
     srow[e] = rows[(int64_t)cc[e / dp4] * dp4 + e % dp4];
   __syncthreads();
+  // the pair distance is symmetric bit for bit and zero on the diagonal, so
+  // the sum over ordered pairs is twice the sum over i < j (wrapping); a
+  // thread takes rows t and R - 1 - t, R - 1 distances in all
   uint32_t sum = 0;
-  for (int i = threadIdx.x; i < R; i += blockDim.x)
-    for (int j = 0; j < R; j++)
-      sum += (uint32_t)(int32_t)sqrtf(dist2_rows_rt(srow + i * dp4, srow + j * dp4, dp4));
+  for (int t = threadIdx.x; t < (R + 1) / 2; t += blockDim.x) {
+    const int i1 = t, i2 = R - 1 - t;
+    for (int j = i1 + 1; j < R; j++)
+      sum += (uint32_t)(int32_t)sqrtf(dist2_rows_rt(srow + i1 * dp4, srow + j * dp4, dp4));
+    if (i2 != i1)
+      for (int j = i2 + 1; j < R; j++)
+        sum += (uint32_t)(int32_t)sqrtf(dist2_rows_rt(srow + i2 * dp4, srow + j * dp4, dp4));
+  }
+  sum *= 2u;
   for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
   __syncthreads();

@@ -50,6 +50,25 @@ def test_selfjoin_integer_clouds_bit_exact(cuda_device, oracle, k):
     np.testing.assert_array_equal(dist, od.astype(np.float32))
 
 
+def test_cloud_with_many_representatives(cuda_device, oracle):
+    """A cloud of 120,000 points gets 1.6 * sqrt(n) = 554 representatives,
+    beyond the 512 that the warp-per-cluster bound kernel takes: that cloud's
+    bounds run on the block kernel, the small clouds' in the same call too."""
+    sizes = [120_000, 3000, 50]
+    pts, off = _int_clouds(sizes, seed=77, span=400)
+    k = 8
+    idx, dist = knnjoin_batched(pts, off, k=k, autotune=False)
+    rows = np.arange(0, sizes[0], 997)
+    oi, od = oracle.bruteforce_f64(pts[:sizes[0]], pts[:sizes[0]], k, qrows=rows)
+    assert np.array_equal(idx[rows], oi)
+    np.testing.assert_array_equal(dist[rows], od.astype(np.float32))
+    for c in (1, 2):
+        a, b = off[c], off[c + 1]
+        oi, od = oracle.bruteforce_f64(pts[a:b], pts[a:b], k)
+        assert np.array_equal(idx[a:b], oi)
+        np.testing.assert_array_equal(dist[a:b], od.astype(np.float32))
+
+
 def test_selfjoin_ellipsoid_clouds(cuda_device, oracle):
     pts, off = data.ellipsoid_clouds(nclouds=60, lo=1, hi=4000, seed=11)
     k = 16
