@@ -6,18 +6,20 @@
 // is an n x R x d GEMM with an arg-max epilogue:
 //     argmax_j  p . r_j - |r_j|^2 / 2
 // computed from BF16-rounded points and representatives with FP32 accumulation
-// in TMEM; the norm term rides in three extra contraction columns.  The choice only has to be approximately nearest: the pruning
-// bounds need the exact distance to whichever representative is chosen, and
-// that distance is recomputed in FP32 afterwards (exact_rep_dist_kernel).
+// in TMEM; the norm term rides in three extra contraction columns.  The
+// choice only has to be approximately nearest: the pruning bounds need the
+// exact distance to whichever representative is chosen, and that distance is
+// recomputed in FP32 afterwards (exact_rep_dist_kernel).
 //
-// One CTA (8 warps) owns 128 points: it converts them to BF16 into shared
-// memory in the core-matrix layout of tc_common.cuh while the first two tiles
-// of TN = 128 representatives (pre-converted once, contiguous) arrive by bulk
-// asynchronous copy; thread 0 issues KD/16 MMAs (M = 128, N = TN, K = 16)
-// per tile into one of two TMEM accumulators and commits to an mbarrier; the
-// warps read the rows back (tcgen05.ld 32x32b) and keep a running arg-max per
-// row while the next tile's MMA runs.  Every wait is bounded; on timeout the
-// CTA flags the error, frees its TMEM and returns.
+// One CTA (8 epilogue warps + 1 producer warp) owns 128 points: all warps
+// convert them to BF16 into shared memory in the core-matrix layout of
+// tc_common.cuh while the first two tiles of TN = 128 representatives
+// (pre-converted once, contiguous) arrive by bulk asynchronous copy; the
+// producer issues KD/16 MMAs (M = 128, N = TN, K = 16) per tile into one of
+// two TMEM accumulators and commits to an mbarrier; the epilogue warps read
+// the rows back (tcgen05.ld 32x32b) and keep a running arg-max per row while
+// the next tile's MMA runs.  Every wait is bounded; on timeout the CTA flags
+// the error, frees its TMEM and returns.
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -329,8 +331,8 @@ int launch_assign_tc(const float4 *rows, int64_t n, int dp4, int d, const float4
                                     cudaFuncAttributePreferredSharedMemoryCarveout,
                                     cudaSharedmemCarveoutMaxShared));
   const int64_t blocks = (n + kTileM - 1) / kTileM;
-  assign_tc_kernel<<<(unsigned)blocks, kAssignThreads, smem, s>>>(rows, n, dp4, d, KD, TN, tiles,
-                                                       Rpad / TN, cl, err);
+  assign_tc_kernel<<<(unsigned)blocks, kAssignThreads, smem, s>>>(rows, n, dp4, d, KD, TN,
+                                                                   tiles, Rpad / TN, cl, err);
   KNN_LAUNCH_CHECK();
   exact_rep_dist_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 32), 256, 0, s>>>(
       rows, n, dp4, reps, cl, dr);
