@@ -240,6 +240,25 @@ int knn_index_free(knn_index *index);
 int knn_index_info(const knn_index *index, int64_t *n, int32_t *d, int32_t *reps);
 
 /*
+ * knn_join over several GPUs of this process, by query ranges.  No
+ * counterpart in the reference, which runs on one GPU (its whole join,
+ * src/knnjoin.cu:983-1172, is what every shard does for its queries).
+ * Host buffers as in knn_join.  The m queries are split into ndev contiguous
+ * ranges as even as the count allows; shard i runs on devices[i] (an id may
+ * repeat: its shards then run concurrently on separate streams) in a host
+ * thread of its own, copies in the n references and its queries, builds the
+ * reference index there (the same options and seed on every device, so the
+ * same index) and joins its queries, writing rows [q0, q0 + m_i) of out_idx /
+ * out_dist.  No data crosses between GPUs.  The result is knn_join's.  stats
+ * (optional): counts summed over the shards, times the slowest shard's
+ * (ms_build includes its index build), qreps_used summed.  Errors: the first
+ * failing shard's code, its message prefixed with the shard and device.
+ */
+int knn_join_sharded(const float *q, int64_t m, const float *r, int64_t n, int32_t d,
+                     int32_t k, int32_t *out_idx, float *out_dist, const knn_options *opt,
+                     const int32_t *devices, int32_t ndev, knn_stats *stats);
+
+/*
  * Returns the device scratch memory the library keeps cached between calls
  * (one stream-ordered pool per device; no reference counterpart: the
  * reference never frees its device memory).  Memory still in use by calls in

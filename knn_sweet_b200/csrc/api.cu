@@ -78,6 +78,27 @@ int scratch_pool(cudaMemPool_t *out) {
   return KNN_OK;
 }
 
+// Argument ranges shared by every entry point.
+int check_sizes(int64_t m, int64_t n, int32_t d, int32_t k) {
+  if (d <= 0) {
+    set_error("d must be positive (got %d)", d);
+    return KNN_EINVAL;
+  }
+  if (k <= 0 || k > KNN_MAX_K) {
+    set_error("k must be in [1, %d] (got %d)", KNN_MAX_K, k);
+    return KNN_EINVAL;
+  }
+  if (m < 0 || n < 0 || m > INT32_MAX || n > INT32_MAX) {
+    set_error("m and n must be in [0, 2^31-1]");
+    return KNN_EINVAL;
+  }
+  if (n > 0 && (int64_t)d > ((int64_t)1 << 40) / n) {
+    set_error("n * d too large");
+    return KNN_EINVAL;
+  }
+  return KNN_OK;
+}
+
 namespace {
 
 // Stream-ordered scratch: every allocation is released on the same stream
@@ -268,25 +289,6 @@ int check_options(const knn_options *opt, knn_options *o) {
   return KNN_OK;
 }
 
-int check_sizes(int64_t m, int64_t n, int32_t d, int32_t k) {
-  if (d <= 0) {
-    set_error("d must be positive (got %d)", d);
-    return KNN_EINVAL;
-  }
-  if (k <= 0 || k > KNN_MAX_K) {
-    set_error("k must be in [1, %d] (got %d)", KNN_MAX_K, k);
-    return KNN_EINVAL;
-  }
-  if (m < 0 || n < 0 || m > INT32_MAX || n > INT32_MAX) {
-    set_error("m and n must be in [0, 2^31-1]");
-    return KNN_EINVAL;
-  }
-  if (n > 0 && (int64_t)d > ((int64_t)1 << 40) / n) {
-    set_error("n * d too large");
-    return KNN_EINVAL;
-  }
-  return KNN_OK;
-}
 
 struct EventSet {
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};

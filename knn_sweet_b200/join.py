@@ -152,6 +152,43 @@ def knnjoin(queries, sources=None, k: int = 200, *, qreps: int = 0, sreps: int =
     return idx, dist
 
 
+def knnjoin_sharded(queries, sources=None, k: int = 200, *, devices=(0,), qreps: int = 0,
+                    sreps: int = 0, seed: int = 2015, rep_trials: int = 10,
+                    precision: str = "fp32", margin: int = 32, stats: bool = False, out=None,
+                    squared: bool = False, tensor_cores: bool = True, lloyd_iters: int = 0):
+    """knnjoin over several GPUs of this process (knn_join_sharded): the queries
+    are split into len(devices) contiguous ranges, each device builds the
+    reference index and joins its range; the result is knnjoin's.  Host
+    (numpy) arrays in and out; a device id may repeat."""
+    lib = _lib.load()
+    opt = _options(qreps, sreps, seed, rep_trials, precision, margin, squared, tensor_cores,
+                   lloyd_iters)
+    st = _lib.KnnStats()
+    q = np.ascontiguousarray(queries, dtype=np.float32)
+    if q.ndim != 2:
+        raise ValueError("queries must be 2-D")
+    r = q if sources is None else np.ascontiguousarray(sources, dtype=np.float32)
+    if r.ndim != 2 or r.shape[1] != q.shape[1]:
+        raise ValueError("sources must be 2-D with the queries' d")
+    m, d = q.shape
+    if out is not None:
+        idx, dist = out
+    else:
+        idx = np.empty((m, k), np.int32)
+        dist = np.empty((m, k), np.float32)
+    dev = np.ascontiguousarray(list(devices), dtype=np.int32)
+    rc = lib.knn_join_sharded(q.ctypes.data_as(ctypes.c_void_p), m,
+                              r.ctypes.data_as(ctypes.c_void_p), r.shape[0], d, k,
+                              idx.ctypes.data_as(ctypes.c_void_p),
+                              dist.ctypes.data_as(ctypes.c_void_p), ctypes.byref(opt),
+                              dev.ctypes.data_as(ctypes.c_void_p), len(dev),
+                              ctypes.byref(st) if stats else None)
+    _lib.check(rc)
+    if stats:
+        return idx, dist, JoinStats(**st.as_dict())
+    return idx, dist
+
+
 def pack_indexdist(idx: np.ndarray, dist: np.ndarray) -> np.ndarray:
     """Interleave into the reference's IndexDist records {int32 index; float dist}."""
     idx = np.ascontiguousarray(idx, dtype=np.int32)

@@ -163,3 +163,27 @@ def test_index_argument_errors_without_gpu():
     assert lib.knn_index_build(None, 10, 3, None, None, None) == _lib.KNN_EINVAL
     assert lib.knn_index_query(None, None, 5, 3, None, None, None, None, None) == _lib.KNN_EINVAL
     assert lib.knn_index_info(None, None, None, None) == _lib.KNN_EINVAL
+
+
+def test_sharded_argument_errors_without_gpu():
+    lib = _lib.load()
+    q = np.zeros((4, 3), np.float32)
+    idx = np.zeros((4, 2), np.int32)
+    dist = np.zeros((4, 2), np.float32)
+    dev = np.zeros(2, np.int32)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    # no device list, or an empty one
+    assert lib.knn_join_sharded(p(q), 4, p(q), 4, 3, 2, p(idx), p(dist), None, None, 2,
+                                None) == _lib.KNN_EINVAL
+    assert lib.knn_join_sharded(p(q), 4, p(q), 4, 3, 2, p(idx), p(dist), None, p(dev), 0,
+                                None) == _lib.KNN_EINVAL
+    assert b"device" in lib.knn_last_error()
+    # bad sizes come first
+    assert lib.knn_join_sharded(p(q), 4, p(q), 4, 3, 0, p(idx), p(dist), None, p(dev), 2,
+                                None) == _lib.KNN_EINVAL
+    # no queries: nothing to do; no references: every slot empty, as knn_join
+    assert lib.knn_join_sharded(None, 0, None, 0, 3, 2, None, None, None, p(dev), 2,
+                                None) == _lib.KNN_OK
+    assert lib.knn_join_sharded(p(q), 4, None, 0, 3, 2, p(idx), p(dist), None, p(dev), 2,
+                                None) == _lib.KNN_OK
+    assert (idx == -1).all() and np.isinf(dist).all()
