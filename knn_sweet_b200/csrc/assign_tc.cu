@@ -9,7 +9,7 @@
 // in TMEM; the norm term rides in three extra contraction columns.  The
 // choice only has to be approximately nearest: the pruning bounds need the
 // exact distance to whichever representative is chosen, and that distance is
-// recomputed in FP32 afterwards (exact_rep_dist_kernel).
+// recomputed in FP32 at the end of the kernel.
 //
 // One CTA (8 epilogue warps + 1 producer warp) owns 128 points: all warps
 // convert them to BF16 into shared memory in the core-matrix layout of
@@ -107,7 +107,8 @@ constexpr int kAssignThreads = 128 * kEsplit + 32;
 __global__ void __launch_bounds__(kAssignThreads, 1)
     assign_tc_kernel(const float4 *__restrict__ rows, int64_t n, int dp4, int d, int KD, int TN,
                      const __nv_bfloat16 *__restrict__ rep_tiles, int ntiles,
-                     int32_t *__restrict__ cl, int *__restrict__ err) {
+                     const float4 *__restrict__ reps, int R, int32_t *__restrict__ cl,
+                     float *__restrict__ dr, int *__restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const size_t a_bytes = tc::tile_bytes(kTileM, KD), b_bytes = tc::tile_bytes(TN, KD);
   unsigned char *sa = smem;
@@ -270,6 +271,8 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
   tc::fence_before_sync();
   __syncthreads();
   const bool ok = *abort_flag == 0;
+  int64_t gr = n;
+  int c = 0;
   if (warp < 4) {
     const int rrow = warp * 32 + lane;
     for (int q = 1; q < kEsplit; q++) {
@@ -277,9 +280,10 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
       const int oi = pi[q * kTileM + rrow];
       if (ov > bv || (ov == bv && oi < bi)) bv = ov, bi = oi;
     }
-    const int64_t gr = row0 + rrow;
+    gr = row0 + rrow;
     // a point whose values are all NaN keeps index 0: a valid cluster
-    if (gr < n) cl[gr] = ok ? bi : 0;
+    c = ok && bi < R ? bi : 0;
+    if (gr < n) cl[gr] = c;
   }
   if (!ok && tid == 0) atomicExch(err, 1);
   if (warp == 0) {
@@ -287,15 +291,9 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
     tc::fence_after_sync();
     tc::tmem_dealloc(tmem, ncols);
   }
-}
-
-// Exact FP32 distance of every point to its chosen representative.
-__global__ void exact_rep_dist_kernel(const float4 *__restrict__ rows, int64_t n, int dp4,
-                                      const float4 *__restrict__ reps,
-                                      const int32_t *__restrict__ cl, float *__restrict__ dr) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    dr[i] = sqrtf(dist2_rows_rt(rows + i * dp4, reps + (int64_t)cl[i] * dp4, dp4));
+  // the exact FP32 distance to the chosen representative, summed in
+  // dimension order with fma (dist2_rows_rt): the only one the bounds use
+  if (gr < n) dr[gr] = sqrtf(dist2_rows_rt(rows + gr * dp4, reps + (int64_t)c * dp4, dp4));
 }
 
 bool assign_tc_supported(int d) { return d >= 16 && d <= 256; }
@@ -331,11 +329,8 @@ int launch_assign_tc(const float4 *rows, int64_t n, int dp4, int d, const float4
                                     cudaFuncAttributePreferredSharedMemoryCarveout,
                                     cudaSharedmemCarveoutMaxShared));
   const int64_t blocks = (n + kTileM - 1) / kTileM;
-  assign_tc_kernel<<<(unsigned)blocks, kAssignThreads, smem, s>>>(rows, n, dp4, d, KD, TN,
-                                                                   tiles, Rpad / TN, cl, err);
-  KNN_LAUNCH_CHECK();
-  exact_rep_dist_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 32), 256, 0, s>>>(
-      rows, n, dp4, reps, cl, dr);
+  assign_tc_kernel<<<(unsigned)blocks, kAssignThreads, smem, s>>>(
+      rows, n, dp4, d, KD, TN, tiles, Rpad / TN, reps, R, cl, dr, err);
   KNN_LAUNCH_CHECK();
   return KNN_OK;
 }
