@@ -320,7 +320,10 @@ struct SelectTopK : TopKBase {
 
   __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int32_t base, int lane) {
     // up to L keys are sorted as they are (their first k are the answer);
-    // beyond that the exact k-th key is selected first
+    // beyond that a tie-inclusive compaction first (every key at or below
+    // the k-th distance stays), and the exact k-th key only if ties still
+    // leave more than L
+    if (nbuf > LL) make_room(lane);
     if (nbuf > LL) flush(lane);
     __syncwarp();
     if constexpr (LL <= 128) {
