@@ -246,7 +246,9 @@ struct SelectTopK : TopKBase {
 
   // A compaction once k + kEarly candidates are in (capacity permitting)
   // tightens the threshold sooner.  k = 200 self-join scan: capacity only
-  // 5.06 ms; kEarly 64: 5.12, 96: 4.94, 128: 4.89, 160: 4.90, 256: 4.97.
+  // 5.06 ms; kEarly 64: 5.12, 96: 4.94, 128: 4.89, 160: 4.90, 256: 4.97
+  // (with the compaction before the end-of-query selection: 96: 4.86,
+  // 128 to 192: 4.76-4.78).
   static constexpr int kEarly = KNN_TOPK_EARLY;
   __device__ __forceinline__ int cap() const { return k + kEarly < kCap ? k + kEarly : kCap; }
 
