@@ -187,3 +187,16 @@ def test_sharded_argument_errors_without_gpu():
     assert lib.knn_join_sharded(p(q), 4, None, 0, 3, 2, p(idx), p(dist), None, p(dev), 2,
                                 None) == _lib.KNN_OK
     assert (idx == -1).all() and np.isinf(dist).all()
+
+
+def test_sharded_python_wrapper_errors_without_gpu():
+    from knn_sweet_b200 import KnnError, knnjoin_sharded
+    x = np.zeros((10, 3), np.float32)
+    with pytest.raises(ValueError):
+        knnjoin_sharded(np.zeros(10, np.float32), None, 2)
+    with pytest.raises(ValueError):
+        knnjoin_sharded(x, np.zeros((5, 4), np.float32), 2)
+    with pytest.raises(KnnError):
+        knnjoin_sharded(x, None, 2, devices=())
+    with pytest.raises(KnnError):
+        knnjoin_sharded(x, None, 0, devices=(0,))
