@@ -411,7 +411,7 @@ def run_forms(torch, dev, flush, steps=3):
         forms[prec] = {"queries_per_s": m / (ms * 1e-3), "ms_per_step": ms,
                        "build_ms": st.ms_build, "search_ms": st.ms_search,
                        "dist_evals_per_query": st.dist_evals / m,
-                       "fp64_rechecks": st.refine_rechecks,
+                       "fp64_rechecks": st.fp64_rechecks,
                        "fallback_queries": st.refine_fallbacks}
     a, b = res["fp32"][0], res["bf16_refine"][0]
     same = (torch.sort(a, 1)[0] == torch.sort(b, 1)[0]).all(1).float().mean().item()

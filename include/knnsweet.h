@@ -13,10 +13,12 @@
  * Conventions
  *  - Points are row-major float32, `d` floats per row, rows packed (stride d).
  *  - Results are structure-of-arrays: out_idx[i*k + j] (int32, 0-based row of
- *    the reference set) and out_dist[i*k + j] (float32 Euclidean distance),
- *    j ascending by (squared distance, index): ties at equal distance go to the
- *    lower reference index.  knn_pack_indexdist() converts to the reference's
- *    interleaved {int index; float dist} layout.
+ *    the reference set) and out_dist[i*k + j] (float32 Euclidean distance).
+ *    The k indices of a query are the k nearest by (FP64 squared distance,
+ *    index) -- exactly the set an FP64 brute-force join gives, ties at equal
+ *    distance going to the lower reference index -- listed ascending by
+ *    (FP32 squared distance, index).  knn_pack_indexdist() converts to the
+ *    reference's interleaved {int index; float dist} layout.
  *  - When fewer than k reference points exist (k > n), the missing slots hold
  *    index -1 and distance +inf (the reference leaves them uninitialised).
  *  - Every call returns 0 (KNN_OK) or a negative KNN_E* code and never exits
@@ -33,7 +35,7 @@
 extern "C" {
 #endif
 
-#define KNNSWEET_ABI_VERSION 1
+#define KNNSWEET_ABI_VERSION 2
 
 /* Status codes (the reference prints and continues: src/knnjoin.cu:38-41). */
 #define KNN_OK 0
@@ -96,7 +98,9 @@ typedef struct knn_stats {
   int64_t pairs_pruned;     /* pairs_total - dist_evals                       */
   int64_t clusters_visited; /* (query, reference cluster) pairs scanned        */
   int64_t clusters_pruned;  /* (query, reference cluster) pairs skipped whole  */
-  int64_t refine_rechecks;  /* BF16 form: candidates re-checked in FP64        */
+  int64_t fp64_rechecks;    /* candidates inside the FP32 rounding band of the
+                               k-th distance whose order was re-decided in FP64
+                               (both forms)                                   */
   int64_t topk_candidates;  /* candidates that beat the running k-th key       */
   int64_t topk_merges;      /* sorted merges of candidate buffers into top-k   */
   float ms_build;           /* representative sampling .. cluster filter      */
@@ -109,6 +113,9 @@ typedef struct knn_stats {
   int32_t refine_fallbacks; /* BF16 form: queries whose kept candidates did
                                not fit the re-ranking buffer and went to the
                                FP32 scan instead                              */
+  int32_t band_queries;     /* queries whose k-th boundary was settled by the
+                               band kernel (a key of the band did not fit the
+                               scan's candidate list)                         */
 } knn_stats;
 
 /* Fill `opt` with the defaults listed above. */
@@ -179,6 +186,10 @@ int knn_backward_device(const float *q, int64_t m, const float *r, int64_t n,
  *    call's contents: calls that overlap on the GPU (different streams, or
  *    host threads racing) corrupt each other.  Serialise them.
  *  - No statistics: the stats-filling path of knn_join_device creates events.
+ *  - Options: qreps, sreps, seed, rep_trials, KNN_SQUARED_DIST and
+ *    KNN_NO_TENSOR_CORES act as for knn_join_device; precision must be
+ *    KNN_FP32 and lloyd_iters 0 (anything else is refused with KNN_EINVAL and
+ *    a message naming the option).
  */
 #define KNN_NOALLOC_SCRATCH_BYTES (32u << 20)
 int knn_join_device_noalloc(const float *q, int64_t m, const float *r, int64_t n,

@@ -50,7 +50,7 @@ class KnnStats(ctypes.Structure):
         ("pairs_pruned", ctypes.c_int64),
         ("clusters_visited", ctypes.c_int64),
         ("clusters_pruned", ctypes.c_int64),
-        ("refine_rechecks", ctypes.c_int64),
+        ("fp64_rechecks", ctypes.c_int64),
         ("topk_candidates", ctypes.c_int64),
         ("topk_merges", ctypes.c_int64),
         ("ms_build", ctypes.c_float),
@@ -60,6 +60,7 @@ class KnnStats(ctypes.Structure):
         ("sreps_used", ctypes.c_int32),
         ("kernels_launched", ctypes.c_int32),
         ("refine_fallbacks", ctypes.c_int32),
+        ("band_queries", ctypes.c_int32),
     ]
 
     def as_dict(self) -> dict:

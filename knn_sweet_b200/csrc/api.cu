@@ -99,6 +99,38 @@ int check_sizes(int64_t m, int64_t n, int32_t d, int32_t k) {
   return KNN_OK;
 }
 
+// Option ranges shared by every entry point.
+int check_options(const knn_options *opt, knn_options *o) {
+  knn_default_options(o);
+  if (opt) *o = *opt;
+  if (o->qreps < 0 || o->sreps < 0 || o->qreps > KNN_MAX_REPS ||
+      o->sreps > KNN_MAX_REPS) {
+    set_error("qreps/sreps must be in [0, %d]", KNN_MAX_REPS);
+    return KNN_EINVAL;
+  }
+  if (o->rep_trials <= 0 || o->rep_trials > 1000) {
+    set_error("rep_trials must be in [1, 1000]");
+    return KNN_EINVAL;
+  }
+  if (o->precision != KNN_FP32 && o->precision != KNN_BF16_REFINE) {
+    set_error("unknown precision %d", o->precision);
+    return KNN_EINVAL;
+  }
+  if (o->margin < 0 || o->margin > 4096) {
+    set_error("margin must be in [0, 4096]");
+    return KNN_EINVAL;
+  }
+  if (o->lloyd_iters < 0 || o->lloyd_iters > 100) {
+    set_error("lloyd_iters must be in [0, 100]");
+    return KNN_EINVAL;
+  }
+  if ((o->flags & ~(KNN_SQUARED_DIST | KNN_NO_TENSOR_CORES)) != 0) {
+    set_error("unknown flags 0x%x", o->flags);
+    return KNN_EINVAL;
+  }
+  return KNN_OK;
+}
+
 namespace {
 
 // Stream-ordered scratch: every allocation is released on the same stream
@@ -151,6 +183,18 @@ class Arena {
     int rc_ = (expr);        \
     if (rc_ != KNN_OK) return rc_; \
   } while (0)
+
+// Device counters of one call, zeroed at its start.
+enum CtrSlot {
+  kCtrWork = 0,                         // scan work counter
+  kCtrScan = 1,                         // the scan statistics (kScanCounters)
+  kCtrErr = kCtrScan + kScanCounters,   // device error flag (bounded waits)
+  kCtrTileWork,                         // tile-search tile counter
+  kCtrTile,                             // tile-search statistics (4)
+  kCtrFallback = kCtrTile + 4,          // slots the tile search leaves to the scan
+  kCtrUnres,                            // queries left to the band kernel
+  kCtrCount
+};
 
 __global__ void fill_empty_kernel(int32_t *idx, float *dist, int64_t count) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
@@ -258,36 +302,6 @@ int build_clusters(Arena &keep, Arena &ar, const float4 *rows, int64_t n, int d,
   return KNN_OK;
 }
 
-int check_options(const knn_options *opt, knn_options *o) {
-  knn_default_options(o);
-  if (opt) *o = *opt;
-  if (o->qreps < 0 || o->sreps < 0 || o->qreps > KNN_MAX_REPS ||
-      o->sreps > KNN_MAX_REPS) {
-    set_error("qreps/sreps must be in [0, %d]", KNN_MAX_REPS);
-    return KNN_EINVAL;
-  }
-  if (o->rep_trials <= 0 || o->rep_trials > 1000) {
-    set_error("rep_trials must be in [1, 1000]");
-    return KNN_EINVAL;
-  }
-  if (o->precision != KNN_FP32 && o->precision != KNN_BF16_REFINE) {
-    set_error("unknown precision %d", o->precision);
-    return KNN_EINVAL;
-  }
-  if (o->margin < 0 || o->margin > 4096) {
-    set_error("margin must be in [0, 4096]");
-    return KNN_EINVAL;
-  }
-  if (o->lloyd_iters < 0 || o->lloyd_iters > 100) {
-    set_error("lloyd_iters must be in [0, 100]");
-    return KNN_EINVAL;
-  }
-  if ((o->flags & ~(KNN_SQUARED_DIST | KNN_NO_TENSOR_CORES)) != 0) {
-    set_error("unknown flags 0x%x", o->flags);
-    return KNN_EINVAL;
-  }
-  return KNN_OK;
-}
 
 
 struct EventSet {
@@ -438,18 +452,17 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
   if (st) KNN_TRY(evs.create());
   KNN_TRY(evs.record(0, s));
   Arena ar(s);
-  // [0] work counter, [1..5] statistics, [6] device error flag, [7] tile
-  // counter, [8..11] tile statistics, [12] count of slots left to the scan
   unsigned long long *ctr;
-  KNN_TRY(ar.alloc(&ctr, 13));
-  KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, 13 * sizeof(unsigned long long), s));
+  KNN_TRY(ar.alloc(&ctr, kCtrCount));
+  KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, kCtrCount * sizeof(unsigned long long), s));
   RefSide R;
-  KNN_TRY(build_ref_side(ar, ar, r, n, d, Rs, o, false, reinterpret_cast<int *>(ctr + 6), s, &R));
+  KNN_TRY(build_ref_side(ar, ar, r, n, d, Rs, o, false, reinterpret_cast<int *>(ctr + kCtrErr),
+                         s, &R));
   return query_impl(R, share, q, m, k, out_idx, out_dist, o, st, s, sink, ar, evs, ctr);
 }
 
-// The query side of a join against a built reference side.  `ctr` (13
-// counters, zeroed) and the events come from the caller; event 0 is recorded.
+// The query side of a join against a built reference side.  `ctr`
+// (kCtrCount counters, zeroed) and the events come from the caller; event 0 is recorded.
 int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t k,
                int32_t *out_idx, float *out_dist, const knn_options &o, knn_stats *st,
                cudaStream_t s, HostSink *sink, Arena &ar, EventSet &evs,
@@ -468,7 +481,7 @@ int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t 
   KNN_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
   const bool self_rows = share;
   const int Rq = share ? Rs : query_rep_count(o, m, d, k, false, Rs);
-  int *dev_err = reinterpret_cast<int *>(ctr + 6);
+  int *dev_err = reinterpret_cast<int *>(ctr + kCtrErr);
   const bool use_tc = (o.flags & KNN_NO_TENSOR_CORES) == 0;
   const float4 *Qp = nullptr;
   ClusterSet qset;
@@ -509,7 +522,7 @@ int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t 
                      tile_search_geometry(d, k, o.margin, num_sms, &grid, &cap, &P, &smem) ==
                          KNN_OK;
   int32_t *fb_slots = nullptr;
-  unsigned *fb_count = reinterpret_cast<unsigned *>(ctr + 12);
+  unsigned *fb_count = reinterpret_cast<unsigned *>(ctr + kCtrFallback);
   if (tiles) {
     grid = (int)std::min<int64_t>(grid, m / 128 + Rq + 1);
     int32_t *tile_list, *ntiles;
@@ -551,11 +564,11 @@ int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t 
     t.buf_pos = buf_pos;
     t.out_idx = out_idx;
     t.out_dist = out_dist;
-    t.work = ctr + 7;
+    t.work = ctr + kCtrTileWork;
     t.fb_slots = fb_slots;
     t.fb_count = fb_count;
     t.err = dev_err;
-    t.counters = ctr + 8;
+    t.counters = ctr + kCtrTile;
     KNN_TRY(launch_tile_search(t, grid, smem, s));
   }
 
@@ -582,10 +595,13 @@ int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t 
   a.rlen = rlen;
   a.Rs = Rs;
   a.n_ref = n;
+  a.rrows = Rp;
   a.out_idx = out_idx;
   a.out_dist = out_dist;
-  a.work_counter = ctr;
-  a.counters = ctr + 1;
+  KNN_TRY(ar.alloc(&a.unres_slot, (size_t)m));
+  a.unres_count = reinterpret_cast<unsigned *>(ctr + kCtrUnres);
+  a.work_counter = ctr + kCtrWork;
+  a.counters = ctr + kCtrScan;
   if (tiles) {
     a.slot_list = fb_slots;
     a.slot_count = fb_count;
@@ -643,21 +659,23 @@ int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t 
   KNN_TRY(evs.record(2, s));
 
   if (st) {
-    unsigned long long h[13];
+    unsigned long long h[kCtrCount];
     KNN_CUDA_TRY(cudaMemcpyAsync(h, ctr, sizeof h, cudaMemcpyDeviceToHost, s));
     KNN_CUDA_TRY(cudaStreamSynchronize(s));
     if (sink && sink->done) KNN_CUDA_TRY(cudaStreamSynchronize(sink->copy));
-    if (static_cast<int>(h[6] & 0xffffffffu) != 0) {
+    if (static_cast<int>(h[kCtrErr] & 0xffffffffu) != 0) {
       set_error("a bounded device wait gave up (tensor-core pipeline)");
       return KNN_ETIMEOUT;
     }
-    st->dist_evals = (int64_t)(h[1] + h[8] + h[9]);
-    st->refine_rechecks = (int64_t)h[10];
-    st->refine_fallbacks = (int32_t)h[11];
-    st->clusters_visited = (int64_t)h[2];
-    st->clusters_pruned = (int64_t)h[3];
-    st->topk_candidates = (int64_t)h[4];
-    st->topk_merges = (int64_t)h[5];
+    const unsigned long long *sc = h + kCtrScan, *tc = h + kCtrTile;
+    st->dist_evals = (int64_t)(sc[0] + tc[0] + tc[1]);
+    st->fp64_rechecks = (int64_t)(sc[5] + tc[2]);
+    st->refine_fallbacks = (int32_t)tc[3];
+    st->band_queries = (int32_t)sc[6];
+    st->clusters_visited = (int64_t)sc[1];
+    st->clusters_pruned = (int64_t)sc[2];
+    st->topk_candidates = (int64_t)sc[3];
+    st->topk_merges = (int64_t)sc[4];
     st->pairs_pruned = st->pairs_total - st->dist_evals;
     st->qreps_used = Rq;
     st->sreps_used = Rs;
@@ -781,8 +799,8 @@ int knn_index_query(const knn_index *index, const float *q, int64_t m, int32_t k
   KNN_TRY(evs.record(0, s));
   Arena ar(s);
   unsigned long long *ctr;
-  KNN_TRY(ar.alloc(&ctr, 13));
-  KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, 13 * sizeof(unsigned long long), s));
+  KNN_TRY(ar.alloc(&ctr, kCtrCount));
+  KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, kCtrCount * sizeof(unsigned long long), s));
   return query_impl(*index->ref, false, q, m, k, out_idx, out_dist, o, st, s, nullptr, ar, evs,
                     ctr);
 }

@@ -453,8 +453,11 @@ int batched_impl(const float *q, const int64_t *qoff_h, const float *r, const in
     BatchArena ar(s);
     unsigned long long *ctr = nullptr;
     auto body = [&]() -> int {
-      KNN_TRY(ar.alloc(&ctr, 7));
-      KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, 7 * sizeof(unsigned long long), s));
+      // [0] scan work counter, [1 ..] scan statistics, then the count of
+      // queries left to the band kernel
+      constexpr int kCtr = 2 + kScanCounters;
+      KNN_TRY(ar.alloc(&ctr, kCtr));
+      KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, kCtr * sizeof(unsigned long long), s));
       if (roff_h[ncloud] == 0) {  // no reference points in any cloud
         batched_fill_empty_kernel<<<148, 256, 0, s>>>(out_idx, out_dist, m * (int64_t)k);
         KNN_LAUNCH_CHECK();
@@ -553,14 +556,17 @@ int batched_impl(const float *q, const int64_t *qoff_h, const float *r, const in
       a.qc_ref_base = qc_ref_base;
       a.Rs = S.Rtot;
       a.n_ref = S.total;
+      a.rrows = S.rows;
       a.out_idx = out_idx;
       a.out_dist = out_dist;
+      KNN_TRY(ar.alloc(&a.unres_slot, (size_t)m));
+      a.unres_count = reinterpret_cast<unsigned *>(ctr + 1 + kScanCounters);
       a.work_counter = ctr;
       a.counters = ctr + 1;
       KNN_TRY(launch_scan(a, num_sms, s));
       if (st) {
         KNN_CUDA_TRY(cudaEventRecord(ev[2], s));
-        unsigned long long h[7];
+        unsigned long long h[kCtr];
         KNN_CUDA_TRY(cudaMemcpyAsync(h, ctr, sizeof h, cudaMemcpyDeviceToHost, s));
         KNN_CUDA_TRY(cudaStreamSynchronize(s));
         st->dist_evals = (int64_t)h[1];
@@ -568,6 +574,8 @@ int batched_impl(const float *q, const int64_t *qoff_h, const float *r, const in
         st->clusters_pruned = (int64_t)h[3];
         st->topk_candidates = (int64_t)h[4];
         st->topk_merges = (int64_t)h[5];
+        st->fp64_rechecks = (int64_t)h[6];
+        st->band_queries = (int32_t)h[7];
         int64_t pairs = 0;
         for (int c = 0; c < ncloud; c++)
           pairs += (qoff_h[c + 1] - qoff_h[c]) * (roff_h[c + 1] - roff_h[c]);

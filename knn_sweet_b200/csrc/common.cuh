@@ -46,6 +46,41 @@ __host__ __device__ __forceinline__ float bound_tol(int d) {
   return (float)(4 * d + 16) * 5.9604645e-8f;
 }
 
+// FP32 rounding band of a k-th squared distance Dk.  A squared distance
+// computed in FP32 (one rounding per difference, the square fused into an
+// fma accumulating non-negative terms in dimension order) is within (d + 2)
+// units of 2^-24 (relative) of the exact value of the same FP32 inputs.  So
+// a point whose FP32 value lies above band_hi(Dk) is farther, exactly and in
+// FP64, than every point at or below Dk, and a point below band_lo(Dk) is
+// nearer than every point at or above Dk: only points inside the band can
+// rank differently in FP32 and in FP64.  The half-width (2d + 12) units covers
+// both values' errors with 8 units to spare for FP64 rounding and the band's
+// own arithmetic (rounded outward).
+__device__ __forceinline__ float band_hi(float D, int d) {
+  return __fmul_ru(D, __fadd_ru(1.0f, (float)(2 * d + 12) * 5.9604645e-8f));
+}
+__device__ __forceinline__ float band_lo(float D, int d) {
+  return __fmul_rd(D, __fsub_rd(1.0f, (float)(2 * d + 12) * 5.9604645e-8f));
+}
+
+// FP64 squared distance of the first d coordinates of two rows, in dimension
+// order, each product and sum rounded separately -- the arithmetic of the
+// FP64 brute-force join the results are checked against.
+__device__ __forceinline__ double dist2_f64(const float *__restrict__ a,
+                                            const float *__restrict__ b, int d) {
+  double acc = 0.0;
+  for (int c = 0; c < d; c++) {
+    const double t = __dsub_rn((double)a[c], (double)b[c]);
+    acc = __dadd_rn(acc, __dmul_rn(t, t));
+  }
+  return acc;
+}
+
+// (FP64 squared distance, index) order: ties go to the lower index.
+__device__ __forceinline__ bool f64_key_less(double da, int32_t ia, double db, int32_t ib) {
+  return da < db || (da == db && ia < ib);
+}
+
 // FP32 squared distance of two padded rows of DP4 float4 (pad lanes are 0 in
 // both rows, so they add exactly 0), summed in dimension order with fma.
 template <int DP4>

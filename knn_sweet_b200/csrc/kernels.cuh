@@ -6,6 +6,12 @@
 
 namespace knnsweet {
 
+// Statistics the scan kernels accumulate (ScanArgs::counters): distance
+// evaluations, clusters visited, clusters pruned, candidates pushed, top-k
+// merges, FP64 distances of the k-th boundary, queries the band kernel
+// settled.
+constexpr int kScanCounters = 7;
+
 // Arguments of the per-query scan.
 struct ScanArgs {
   const float4 *qrows;      // m x dp4, original query order
@@ -33,10 +39,15 @@ struct ScanArgs {
   int Rs;
   int64_t n_ref;            // reference points (0: unknown); with Rs it gives
                             // the mean cluster size the scan variant is chosen by
+  const float4 *rrows;      // n x dp4 reference rows, original order (the
+                            // FP64 re-check of the k-th boundary)
   int32_t *out_idx;         // m x k
   float *out_dist;          // m x k
+  int32_t *unres_slot;      // room for every slot of the launch: queries
+                            // whose boundary the band kernel settles ...
+  unsigned *unres_count;    // ... and their number (zeroed by launch_scan)
   unsigned long long *work_counter;  // zeroed before launch
-  unsigned long long *counters;      // [evals, visited, pruned, pushed, merges]
+  unsigned long long *counters;      // kScanCounters statistics (or null)
 };
 
 int launch_pack_rows(const float *src, int64_t n, int d, int dp4, float4 *dst,

@@ -9,11 +9,13 @@
 // owns its inputs and outputs; everything else the join needs lives in one
 // fixed array compiled into this library.
 //
-// The join is the same pipeline as knn_join_device (same kernels, same
-// launch order, same results); only the origin of the scratch differs: every
-// buffer is carved from `g_static_scratch` instead of the stream-ordered
-// pool, and the representative draw reaches the device as kernel parameters,
-// so no host heap is touched either.
+// The join is knn_join_device's plain FP32 pipeline with the reference's
+// representative draw (same kernels, same launch order, same results); only
+// the origin of the scratch differs: every buffer is carved from
+// `g_static_scratch` instead of the stream-ordered pool, and the draw reaches
+// the device as kernel parameters, so no host heap is touched either.  The
+// BF16 form and the representative refinement are refused (their buffers
+// scale with options this array cannot promise).
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
@@ -28,6 +30,10 @@
 static __device__ __align__(256) unsigned char g_static_scratch[KNN_NOALLOC_SCRATCH_BYTES];
 
 namespace knnsweet {
+
+int check_sizes(int64_t m, int64_t n, int32_t d, int32_t k);
+int check_options(const knn_options *opt, knn_options *o);
+
 namespace {
 
 // Device address of g_static_scratch per device.  In host code the symbol
@@ -90,24 +96,31 @@ struct SideBufs {
   int32_t *vals = nullptr, *perm = nullptr;
   unsigned char *temp = nullptr;
   size_t temp_bytes = 0;
+  unsigned char *tc = nullptr;  // tensor-core assignment scratch (d >= 16)
   int32_t *off = nullptr;
 };
+
+// Device counters: [0] scan work counter, [1 ..] scan statistics, then the
+// count of queries left to the band kernel and the device error flag.
+constexpr int kCtrUnres = 1 + kScanCounters, kCtrErr = kCtrUnres + 1, kCtrCount = kCtrErr + 1;
 
 struct Plan {
   int64_t m = 0, n = 0;
   int d = 0, k = 0, dp4s = 0, tmpl = 0, Rq = 0, Rs = 0, trials = 0;
   uint32_t seed = 0;
-  bool share = false, pack_r = false, pack_q = false, idx_in_row = false;
+  bool share = false, pack_r = false, pack_q = false, idx_in_row = false, use_tc = false;
   SideBufs S, Q;
   float4 *srows = nullptr;
   float *sdist = nullptr, *cmin = nullptr, *cmax = nullptr;
   int32_t *sidx = nullptr;
   float *qrad = nullptr, *drr = nullptr, *theta0 = nullptr;
   int32_t *slot_cl = nullptr, *rlist = nullptr, *rlen = nullptr;
+  int32_t *unres = nullptr;
   unsigned long long *ctr = nullptr;
 };
 
-void carve_side(Carver &c, SideBufs &b, int64_t n, int dp4s, int R, int trials, bool pack) {
+void carve_side(Carver &c, SideBufs &b, int64_t n, int d, int dp4s, int R, int trials, bool pack,
+                bool use_tc) {
   b.packed = pack ? c.take<float4>(n * dp4s) : nullptr;
   b.cand = c.take<int32_t>((int64_t)trials * R);
   b.score = c.take<uint32_t>(trials);
@@ -121,24 +134,26 @@ void carve_side(Carver &c, SideBufs &b, int64_t n, int dp4s, int R, int trials, 
   b.perm = c.take<int32_t>(n);
   b.temp_bytes = cluster_sort_temp_bytes(n, R);
   b.temp = c.take<unsigned char>((int64_t)b.temp_bytes);
+  b.tc = use_tc ? c.take<unsigned char>((int64_t)assign_tc_scratch_bytes(R, d)) : nullptr;
   b.off = c.take<int32_t>((int64_t)R + 1);
 }
 
 void carve(Carver &c, Plan &p) {
-  carve_side(c, p.S, p.n, p.dp4s, p.Rs, p.trials, p.pack_r);
+  carve_side(c, p.S, p.n, p.d, p.dp4s, p.Rs, p.trials, p.pack_r, p.use_tc);
   p.srows = c.take<float4>(p.n * p.dp4s);
   p.sdist = c.take<float>(p.n);
   p.sidx = c.take<int32_t>(p.n);
   p.cmin = c.take<float>(p.Rs);
   p.cmax = c.take<float>(p.Rs);
-  if (!p.share) carve_side(c, p.Q, p.m, p.dp4s, p.Rq, p.trials, p.pack_q);
+  if (!p.share) carve_side(c, p.Q, p.m, p.d, p.dp4s, p.Rq, p.trials, p.pack_q, p.use_tc);
   p.qrad = c.take<float>(p.Rq);
   p.slot_cl = c.take<int32_t>(p.m);
   p.drr = c.take<float>((int64_t)p.Rq * p.Rs);
   p.theta0 = c.take<float>(p.Rq);
   p.rlist = c.take<int32_t>((int64_t)p.Rq * p.Rs);
   p.rlen = c.take<int32_t>(p.Rq);
-  p.ctr = c.take<unsigned long long>(6);
+  p.unres = c.take<int32_t>(p.m);
+  p.ctr = c.take<unsigned long long>(kCtrCount);
 }
 
 // The representative draw travels as kernel parameters, 8,000 indices per
@@ -187,7 +202,13 @@ int cluster_side(const Plan &p, const SideBufs &b, const float *src, int64_t n, 
   int rc = draw_reps(b, n, R, p.trials, p.seed, s);
   if (rc == KNN_OK)
     rc = launch_rep_select(rows, p.dp4s, b.cand, R, p.trials, b.score, b.reps, b.rep_rows, s);
-  if (rc == KNN_OK) rc = launch_assign(rows, n, p.dp4s, b.reps, R, b.cl, b.dr, s);
+  if (rc == KNN_OK) {
+    if (b.tc)
+      rc = launch_assign_tc(rows, n, p.dp4s, p.d, b.reps, R, b.tc, b.cl, b.dr,
+                            reinterpret_cast<int *>(p.ctr + kCtrErr), s);
+    else
+      rc = launch_assign(rows, n, p.dp4s, b.reps, R, b.cl, b.dr, s);
+  }
   if (rc == KNN_OK)
     rc = launch_cluster_sort(b.cl, b.dr, n, R, b.keys, b.vals, b.skeys, b.perm, b.temp,
                              b.temp_bytes, s);
@@ -205,18 +226,17 @@ int noalloc_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d
                  int32_t *out_idx, float *out_dist, const knn_options *opt,
                  cudaStream_t s) {
   knn_options o;
-  knn_default_options(&o);
-  if (opt) o = *opt;
-  if (d <= 0 || k <= 0 || k > KNN_MAX_K || m < 0 || n < 0 || m > INT32_MAX ||
-      n > INT32_MAX) {
-    set_error("bad sizes: need d > 0, 1 <= k <= %d, 0 <= m, n < 2^31", KNN_MAX_K);
+  int rc = check_options(opt, &o);
+  if (rc == KNN_OK) rc = check_sizes(m, n, d, k);
+  if (rc != KNN_OK) return rc;
+  if (o.precision != KNN_FP32) {
+    set_error("knn_join_device_noalloc: precision must be KNN_FP32 (the BF16 form's "
+              "candidate buffers grow with k and margin beyond the fixed scratch)");
     return KNN_EINVAL;
   }
-  if (o.qreps < 0 || o.sreps < 0 || o.qreps > KNN_MAX_REPS || o.sreps > KNN_MAX_REPS ||
-      o.rep_trials <= 0 || o.rep_trials > 1000 || o.flags != 0 ||
-      (o.precision != KNN_FP32 && o.precision != KNN_BF16_REFINE) || o.margin < 0 ||
-      o.margin > 4096) {
-    set_error("bad options");
+  if (o.lloyd_iters != 0) {
+    set_error("knn_join_device_noalloc: lloyd_iters must be 0 (representative refinement "
+              "is only available through knn_join_device)");
     return KNN_EINVAL;
   }
   launch_counter() = 0;
@@ -257,6 +277,7 @@ int noalloc_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d
   };
   p.pack_r = needs_pack(r);
   p.pack_q = needs_pack(q);
+  p.use_tc = (o.flags & KNN_NO_TENSOR_CORES) == 0 && assign_tc_supported(d);
 
   // size check before anything touches the array
   Carver measure(nullptr);
@@ -269,7 +290,7 @@ int noalloc_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d
     return KNN_EINVAL;
   }
   unsigned char *base = nullptr;
-  int rc = static_scratch(&base);
+  rc = static_scratch(&base);
   if (rc != KNN_OK) return rc;
   Carver carver(base);
   carve(carver, p);
@@ -278,6 +299,10 @@ int noalloc_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d
   KNN_CUDA_TRY(cudaGetDevice(&dev));
   KNN_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
 
+  // the array keeps the previous call's contents: the counters (work
+  // counter, statistics, band list length, error flag) must start at zero;
+  // every other buffer is written before it is read
+  KNN_CUDA_TRY(cudaMemsetAsync(p.ctr, 0, kCtrCount * sizeof(unsigned long long), s));
   const float4 *Rp = nullptr, *Qp = nullptr;
   rc = cluster_side(p, p.S, r, n, p.Rs, &Rp, s);
   if (rc != KNN_OK) return rc;
@@ -298,10 +323,6 @@ int noalloc_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d
     rc = launch_bounds_filter(p.drr, p.Rq, p.Rs, p.qrad, Qb.off, p.S.off, p.sdist, p.cmax,
                               k, d, p.theta0, p.rlist, p.rlen, s);
   if (rc != KNN_OK) return rc;
-  // the array keeps the previous call's contents: the work counter and the
-  // statistics must start at zero (every other buffer is written before it
-  // is read)
-  KNN_CUDA_TRY(cudaMemsetAsync(p.ctr, 0, 6 * sizeof(unsigned long long), s));
   ScanArgs a{};
   a.qrows = Qp;
   a.qorder = Qb.perm;
@@ -312,6 +333,7 @@ int noalloc_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d
   a.dp4_tmpl = p.tmpl;
   a.k = k;
   a.idx_in_row = p.idx_in_row;
+  a.squared = (o.flags & KNN_SQUARED_DIST) != 0;
   a.sreps = p.S.reps;
   a.srows = p.srows;
   a.sdist = p.sdist;
@@ -323,8 +345,12 @@ int noalloc_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d
   a.rlist = p.rlist;
   a.rlen = p.rlen;
   a.Rs = p.Rs;
+  a.n_ref = n;
+  a.rrows = Rp;
   a.out_idx = out_idx;
   a.out_dist = out_dist;
+  a.unres_slot = p.unres;
+  a.unres_count = reinterpret_cast<unsigned *>(p.ctr + kCtrUnres);
   a.work_counter = p.ctr;
   a.counters = p.ctr + 1;
   return launch_scan(a, num_sms, s);

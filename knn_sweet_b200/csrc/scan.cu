@@ -37,29 +37,58 @@
 
 namespace knnsweet {
 
-// Shared part of both top-k variants: the append buffer and the threshold.
+// Shared part of the top-k variants: the append buffer, the admission
+// threshold and what the FP64 re-check of the k-th boundary needs.
+//
+// The neighbour set must be the one an FP64 join gives.  Keys are FP32
+// (d^2, index) words, which rank two points differently from FP64 only when
+// both lie inside the FP32 rounding band of the k-th squared distance
+// (band_lo / band_hi).  So the admission threshold, once k keys are in, is
+// band_hi of the current k-th value (every point that may still belong to
+// the final band is admitted and never pruned), compactions keep every key up
+// to that value, and `lostmin` records the smallest FP32 d^2 of any key that
+// had to be dropped for lack of room while it could still lie in the final
+// band.  At the end of the query the band is re-decided in FP64
+// (band_resolve_fp64); a query that lost a band key goes to the band kernel
+// instead.
 struct TopKBase {
   uint64_t *buf;  // append buffer (shared memory)
-  int nbuf, nlist, k;
+  int nbuf, nlist, k, d;
   uint64_t thr;   // a candidate enters iff its key < thr
   float theta;    // distance matching thr (bound for the pruning tests)
+  float lostmin;  // smallest FP32 d^2 dropped for lack of room (+inf: none)
   unsigned pushed = 0, merges = 0;  // statistics of the current query (warp-uniform)
 
   __device__ __forceinline__ void reset_threshold(float th0) {
     nbuf = 0;
     nlist = 0;
     theta = th0;
+    lostmin = __int_as_float(0x7f800000);
     // admits every d^2 <= th0^2, whatever the index
     thr = ((uint64_t)__float_as_uint(th0 * th0) << 32) | 0xffffffffull;
   }
+  // threshold once the k-th squared distance is T: the FP32 band above it
+  __device__ __forceinline__ void set_band_threshold(float T) {
+    const float W = band_hi(T, d);
+    thr = ((uint64_t)__float_as_uint(W) << 32) | 0xffffffffull;
+    theta = sqrtf(W);
+  }
+  // a dropped key's distance word (NaN from an empty key is ignored)
+  __device__ __forceinline__ void note_lost(uint32_t d2bits) {
+    lostmin = fminf(lostmin, __uint_as_float(__reduce_min_sync(kFull, d2bits)));
+  }
 };
 
-// k <= 256: the sorted list of the best keys lives in registers.
+// Small k: the sorted list of the best keys lives in registers
+// (one key per lane), with the FP32 band of the k-th kept behind it as far as
+// the 32 slots allow.
 template <int E>
 struct RegTopK : TopKBase {
   static constexpr int L = 32 * E;
-  static constexpr int kCap = L;       // candidate buffer capacity
-  static constexpr int kSmemKeys = L;  // per warp
+  static constexpr int kCap = L;  // candidate buffer capacity
+  // append buffer (L keys), L doubles for the FP64 band, 2 pivot words
+  static constexpr int kSmemKeys = 2 * L + 2;
+  static constexpr int kBandScratch = L, kPivot = 2 * L;
   uint64_t v[E];
 
   __device__ __forceinline__ int cap() const { return kCap; }
@@ -88,40 +117,47 @@ struct RegTopK : TopKBase {
     __syncwarp();
     reg_bitonic_sort<E>(b, lane);
     // v ascending, b ascending: min(v[i], b[L-1-i]) holds the L smallest of
-    // both as a bitonic sequence.
+    // both as a bitonic sequence; the larger of each pair is dropped
+    uint32_t lost = 0xffffffffu;
 #pragma unroll
-    for (int j = 0; j < E; j++) v[j] = umin64(v[j], shfl64(b[E - 1 - j], 31 - lane));
+    for (int j = 0; j < E; j++) {
+      const uint64_t o = shfl64(b[E - 1 - j], 31 - lane);
+      lost = min(lost, (uint32_t)(umax64(v[j], o) >> 32));
+      v[j] = umin64(v[j], o);
+    }
+    note_lost(lost);
     reg_bitonic_merge<E>(v, lane);
     nlist = min(k, nlist + nbuf);
     merges++;
     nbuf = 0;
-#pragma unroll
-    for (int j = 0; j < E; j++)
-      if (E * lane + j >= k) v[j] = kKeyMax;
     if (nlist == k) {
       const int kl = (k - 1) / E, kj = (k - 1) % E;
       uint64_t mine = kKeyMax;
 #pragma unroll
       for (int j = 0; j < E; j++)
         if (j == kj) mine = v[j];
-      thr = shfl64(mine, kl);
-      theta = sqrtf(key_d2(thr));
+      const float T = key_d2(shfl64(mine, kl));
+      // keys behind the k-th stay only inside its band (the ones dropped
+      // here are above band_hi of a k-th that can only fall)
+      const float hi = band_hi(T, d);
+#pragma unroll
+      for (int j = 0; j < E; j++)
+        if (E * lane + j >= k && key_d2(v[j]) > hi) v[j] = kKeyMax;
+      set_band_threshold(T);
     }
   }
 
-  // Writes the k results (through the buffer for coalesced stores).
-  __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int32_t base, int lane) {
+  // The candidates, sorted, into buf[0..n); returns n.
+  __device__ __forceinline__ int sorted(int lane) {
     __syncwarp();
+    int n = 0;
 #pragma unroll
-    for (int j = 0; j < E; j++) buf[E * lane + j] = v[j];
-    __syncwarp();
-    for (int t = lane; t < k; t += 32) {
-      const uint64_t key = buf[t];
-      const bool none = key == kKeyMax;
-      oi[t] = none ? -1 : key_idx(key) - base;
-      od[t] = none ? __int_as_float(0x7f800000) : (squared ? key_d2(key) : sqrtf(key_d2(key)));
+    for (int j = 0; j < E; j++) {
+      buf[E * lane + j] = v[j];
+      n += __popc(__ballot_sync(kFull, v[j] != kKeyMax));
     }
     __syncwarp();
+    return n;
   }
 };
 
@@ -151,87 +187,9 @@ __device__ __forceinline__ void smem_bitonic_sort(uint64_t *s, int lane) {
   }
 }
 
-template <int L>
-__device__ __forceinline__ void smem_bitonic_merge(uint64_t *s, int lane) {
-#pragma unroll 1
-  for (int stride = L >> 1; stride > 0; stride >>= 1) {
-#pragma unroll
-    for (int t0 = 0; t0 < (L / 2 + 31) / 32; t0++) {
-      const int t = t0 * 32 + lane;
-      if (t < L / 2) {
-        const int i = 2 * t - (t & (stride - 1));
-        const int j = i + stride;
-        const uint64_t a = s[i], b = s[j];
-        if (a > b) {
-          s[i] = b;
-          s[j] = a;
-        }
-      }
-    }
-    __syncwarp();
-  }
-}
-
-// k > 256: list and buffer both in shared memory.
-template <int LL>
-struct SmemTopK : TopKBase {
-  static constexpr int L = LL;
-  static constexpr int kCap = L;
-  static constexpr int kSmemKeys = 2 * L;
-  uint64_t *list;
-
-  __device__ __forceinline__ int cap() const { return kCap; }
-
-  __device__ __forceinline__ void init(uint64_t *wsm) {
-    list = wsm;
-    buf = wsm + L;
-  }
-
-  __device__ __forceinline__ void reset(float th0, int lane) {
-    __syncwarp();
-    for (int i = lane; i < L; i += 32) list[i] = kKeyMax;
-    reset_threshold(th0);
-    __syncwarp();
-  }
-
-  __device__ __forceinline__ void make_room(int lane) { flush(lane); }
-  // end of the query: pending candidates merged into the list
-  __device__ __forceinline__ void finish(int lane) { flush(lane); }
-
-  __device__ __forceinline__ void flush(int lane) {
-    if (nbuf == 0) return;
-    __syncwarp();
-    for (int i = nbuf + lane; i < L; i += 32) buf[i] = kKeyMax;
-    __syncwarp();
-    smem_bitonic_sort<L>(buf, lane);
-    for (int i = lane; i < L; i += 32) list[i] = umin64(list[i], buf[L - 1 - i]);
-    __syncwarp();
-    smem_bitonic_merge<L>(list, lane);
-    nlist = min(k, nlist + nbuf);
-    merges++;
-    nbuf = 0;
-    for (int i = k + lane; i < L; i += 32) list[i] = kKeyMax;
-    __syncwarp();
-    if (nlist == k) {
-      thr = list[k - 1];
-      theta = sqrtf(key_d2(thr));
-    }
-  }
-
-  __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int32_t base, int lane) {
-    for (int t = lane; t < k; t += 32) {
-      const uint64_t key = list[t];
-      const bool none = key == kKeyMax;
-      oi[t] = none ? -1 : key_idx(key) - base;
-      od[t] = none ? __int_as_float(0x7f800000) : (squared ? key_d2(key) : sqrtf(key_d2(key)));
-    }
-    __syncwarp();
-  }
-};
-
 // Top-k as an unsorted candidate set in shared memory (capacity 2L).  When it
-// fills, the exact k-th key is found by warp_select_kth, the set is compacted
-// to the k best and the threshold drops to that key; the k results are sorted
+// fills, the k-th smallest squared distance T is found by a radix selection
+// and the set keeps every key up to band_hi(T); the k results are sorted
 // once, at the end of the query.
 #ifndef KNN_TOPK_EARLY
 #define KNN_TOPK_EARLY 160
@@ -242,6 +200,9 @@ struct SelectTopK : TopKBase {
   static constexpr int L = LL;          // final sort length (pow2 >= k)
   static constexpr int kCap = 2 * LL;   // candidate capacity
   static constexpr int kSmemKeys = 2 * LL + 128;  // keys + 256-word histogram
+  // after the final sort: LL doubles for the FP64 band behind the sorted
+  // keys, the pivot in the histogram's words
+  static constexpr int kBandScratch = LL, kPivot = 2 * LL;
   uint32_t *hist;
 
   // A compaction once k + kEarly candidates are in (capacity permitting)
@@ -259,46 +220,50 @@ struct SelectTopK : TopKBase {
 
   __device__ __forceinline__ void reset(float th0, int) { reset_threshold(th0); }
 
-  // Reduce the set to its k smallest keys (no-op with k or fewer).
+  // Reduce the set to its k smallest keys (no-op with k or fewer) when ties
+  // leave no room otherwise; the keys it drops go into lostmin.
   __device__ __forceinline__ void flush(int lane) {
     if (nbuf <= k) return;
     __syncwarp();
     const uint64_t kth = warp_select_kth(buf, nbuf, k, hist, lane);
     __syncwarp();
     int w = 0;
+    uint32_t lost = 0xffffffffu;
     for (int b0 = 0; b0 < nbuf; b0 += 32) {
       const int i = b0 + lane;
       const uint64_t v = i < nbuf ? buf[i] : kKeyMax;
       const bool keep = i < nbuf && v <= kth;
+      if (i < nbuf && !keep) lost = min(lost, (uint32_t)(v >> 32));
       const unsigned bm = __ballot_sync(kFull, keep);
       __syncwarp();
       if (keep) buf[w + __popc(bm & ((1u << lane) - 1))] = v;
       w += __popc(bm);
     }
     __syncwarp();
+    note_lost(lost);
     nbuf = w;  // == k
     nlist = k;
     merges++;
-    thr = kth;
-    theta = sqrtf(key_d2(thr));
+    set_band_threshold(key_d2(kth));
   }
 
   // Room for more candidates while the query runs: keep every key whose
-  // squared distance is at most the k-th smallest one -- at least k keys,
-  // ties included -- found by a 32-bit selection on the keys' distance words
-  // (on data with many equal distances the 64-bit selection spends most of
-  // its passes on the index bits of the ties).  The exact k-th key is only
-  // needed at the end (flush).  Falls back to it when ties fill the buffer.
+  // squared distance is at most band_hi of the k-th smallest one T -- at
+  // least k keys, ties and the FP32 band included -- found by a 32-bit
+  // selection on the keys' distance words (on data with many equal distances
+  // a 64-bit selection spends most of its passes on the index bits of the
+  // ties).  Falls back to the exact k-key flush when ties fill the buffer.
   __device__ __forceinline__ void make_room(int lane) {
     if (nbuf <= k) return;
     __syncwarp();
     const uint32_t T = warp_select_kth_u32(reinterpret_cast<const uint32_t *>(buf) + 1, 2,
                                            nbuf, k, hist, lane);
+    const uint32_t W = __float_as_uint(band_hi(__uint_as_float(T), d));
     int w = 0;
     for (int b0 = 0; b0 < nbuf; b0 += 32) {
       const int i = b0 + lane;
       const uint64_t v = i < nbuf ? buf[i] : kKeyMax;
-      const bool keep = i < nbuf && (uint32_t)(v >> 32) <= T;
+      const bool keep = i < nbuf && (uint32_t)(v >> 32) <= W;
       const unsigned bm = __ballot_sync(kFull, keep);
       __syncwarp();
       if (keep) buf[w + __popc(bm & ((1u << lane) - 1))] = v;
@@ -311,20 +276,17 @@ struct SelectTopK : TopKBase {
       return;
     }
     merges++;
-    thr = ((uint64_t)T << 32) | 0xffffffffull;
-    theta = sqrtf(__uint_as_float(T));
+    nlist = k;
+    set_band_threshold(__uint_as_float(T));
   }
 
-  // End of the query: nothing to do -- write_out sorts up to L keys as they
-  // are (their first k are the answer) and selects the exact k-th key first
-  // only beyond that, which saves the 64-bit selection for most queries.
+  // End of the query: nothing to do before sorted().
   __device__ __forceinline__ void finish(int) {}
 
-  __device__ __forceinline__ void write_out(int32_t *oi, float *od, bool squared, int32_t base, int lane) {
-    // up to L keys are sorted as they are (their first k are the answer);
-    // beyond that a tie-inclusive compaction first (every key at or below
-    // the k-th distance stays), and the exact k-th key only if ties still
-    // leave more than L
+  // The candidates, sorted, into buf[0..n); returns n.  Up to L keys are
+  // sorted as they are; beyond that a band-inclusive compaction first, and
+  // the exact k-key flush only if ties still leave more than L.
+  __device__ __forceinline__ int sorted(int lane) {
     if (nbuf > LL) make_room(lane);
     if (nbuf > LL) flush(lane);
     __syncwarp();
@@ -343,27 +305,14 @@ struct SelectTopK : TopKBase {
       __syncwarp();
       reg_bitonic_sort<E>(x, lane);
 #pragma unroll
-      for (int j = 0; j < E; j++) {
-        const int t = E * lane + j;
-        if (t < k) {
-          const bool none = x[j] == kKeyMax;
-          oi[t] = none ? -1 : key_idx(x[j]) - base;
-          od[t] = none ? __int_as_float(0x7f800000)
-                       : (squared ? key_d2(x[j]) : sqrtf(key_d2(x[j])));
-        }
-      }
+      for (int j = 0; j < E; j++) buf[E * lane + j] = x[j];
     } else {
       for (int i = nbuf + lane; i < LL; i += 32) buf[i] = kKeyMax;
       __syncwarp();
       smem_bitonic_sort<LL>(buf, lane);
-      for (int t = lane; t < k; t += 32) {
-        const uint64_t key = buf[t];
-        const bool none = key == kKeyMax;
-        oi[t] = none ? -1 : key_idx(key) - base;
-        od[t] = none ? __int_as_float(0x7f800000) : (squared ? key_d2(key) : sqrtf(key_d2(key)));
-      }
     }
     __syncwarp();
+    return nbuf;
   }
 };
 
@@ -383,6 +332,109 @@ __device__ __forceinline__ void topk_push(TK &tk, uint64_t key, int lane) {
   if (pass) tk.buf[tk.nbuf + __popc(b & ((1u << lane) - 1))] = key;
   tk.nbuf += cnt;
   tk.pushed += cnt;
+}
+
+// FP64 re-decision of one query's k-th boundary, by one warp.  s[0..n) holds
+// the query's candidate keys sorted ascending, n > k; s[0..nlo) lie below the
+// FP32 band of the k-th (band_lo(Dk) .. band_hi(Dk)), s[nlo..nhi) inside it,
+// nhi > k, and every point inside the band is among them.  Keys below the
+// band are in the FP64 top k, keys above it are not; the band's keys are
+// ranked by (FP64 d^2, index) and the best k - nlo of them kept in place, in
+// their FP32 order, so that s[0..k) is the FP64 join's neighbour set.  (The
+// reference decides this boundary by a strict-less insertion of FP32
+// distances, src/knnjoin.cu:815-820.)  qf: the query row; rrows: the
+// reference rows in original order (keys carry original indices); dbl:
+// scratch for nhi - nlo doubles; piv: 2 words.  Out of line: it runs for few
+// queries, and inlined it would cost the scan registers.
+__device__ __noinline__ void band_resolve_fp64(uint64_t *s, int nlo, int nhi, int k, int d,
+                                               int dp4, const float *__restrict__ qf,
+                                               const float4 *__restrict__ rrows, double *dbl,
+                                               uint64_t *piv, int lane) {
+  const int nb = nhi - nlo, need = k - nlo;
+  for (int e = lane; e < nb; e += 32) {
+    const int32_t id = key_idx(s[nlo + e]);
+    dbl[e] = dist2_f64(qf, reinterpret_cast<const float *>(rrows + (int64_t)id * dp4), d);
+  }
+  __syncwarp();
+  // the need-th smallest (FP64 d^2, index) of the band (ranks are distinct)
+  for (int e = lane; e < nb; e += 32) {
+    const double de = dbl[e];
+    const int32_t ie = key_idx(s[nlo + e]);
+    int rank = 0;
+    for (int f = 0; f < nb; f++) rank += f64_key_less(dbl[f], key_idx(s[nlo + f]), de, ie);
+    if (rank == need - 1) {
+      piv[0] = (uint64_t)__double_as_longlong(de);
+      piv[1] = (uint64_t)(uint32_t)ie;
+    }
+  }
+  __syncwarp();
+  const double pd = __longlong_as_double((long long)piv[0]);
+  const int32_t pi = (int32_t)piv[1];
+  // keep the band's keys up to the pivot, in place, order preserved
+  int w = nlo;
+  for (int b0 = 0; b0 < nb; b0 += 32) {
+    const int e = b0 + lane;
+    const uint64_t key = e < nb ? s[nlo + e] : kKeyMax;
+    const bool keep = e < nb && !f64_key_less(pd, pi, dbl[e], key_idx(key));
+    const unsigned bm = __ballot_sync(kFull, keep);
+    __syncwarp();
+    if (keep) s[w + __popc(bm & ((1u << lane) - 1))] = key;
+    w += __popc(bm);
+  }
+  __syncwarp();
+}
+
+// End of one query of the warp scan: sorts the candidates, settles the k-th
+// boundary in FP64 (or, when a key of its band was dropped for lack of room,
+// hands the query to the band kernel: the last output slot then carries the
+// number of keys below the band and the FP32 k-th value), writes the k
+// results.  Returns the FP64 distances evaluated.
+template <class TK>
+__device__ __forceinline__ unsigned emit_query(TK &tk, const ScanArgs &a, int32_t slot, int64_t q,
+                                               int qc, int lane) {
+  const int n = tk.sorted(lane);
+  uint64_t *s = tk.buf;
+  const int k = a.k;
+  bool defer = false;
+  int nlo = 0;
+  float Dk = 0.0f;
+  unsigned checked = 0;
+  if (n >= k) {
+    Dk = key_d2(s[k - 1]);
+    const float lo = band_lo(Dk, a.d), hi = band_hi(Dk, a.d);
+    int nhi = 0;
+    for (int b0 = 0; b0 < n; b0 += 32) {
+      const int e = b0 + lane;
+      const float v = e < n ? key_d2(s[e]) : __int_as_float(0x7f800000);
+      nlo += __popc(__ballot_sync(kFull, v < lo));
+      nhi += __popc(__ballot_sync(kFull, v <= hi));
+    }
+    if (tk.lostmin <= hi) {
+      defer = true;
+    } else if (nhi > k) {
+      band_resolve_fp64(s, nlo, nhi, k, a.d, a.dp4,
+                        reinterpret_cast<const float *>(a.qrows + q * a.dp4), a.rrows,
+                        reinterpret_cast<double *>(s + TK::kBandScratch), s + TK::kPivot, lane);
+      checked = (unsigned)(nhi - nlo);
+    }
+  }
+  int32_t *oi = a.out_idx + q * k;
+  float *od = a.out_dist + q * k;
+  const int32_t base = a.qc_ref_base ? (int32_t)a.qc_ref_base[qc] : 0;
+  for (int t = lane; t < k; t += 32) {
+    const uint64_t key = t < n ? s[t] : kKeyMax;
+    const bool none = key == kKeyMax;
+    if (defer && t == k - 1) {
+      oi[t] = nlo;
+      od[t] = Dk;
+    } else {
+      oi[t] = none ? -1 : key_idx(key) - base;
+      od[t] = none ? __int_as_float(0x7f800000) : (a.squared ? key_d2(key) : sqrtf(key_d2(key)));
+    }
+  }
+  if (defer && lane == 0) a.unres_slot[atomicAdd(a.unres_count, 1u)] = slot;
+  __syncwarp();
+  return checked;
 }
 
 // ---------------------------------------------------------------------------
@@ -440,13 +492,13 @@ struct QueryRow<0, IDXROW> {
 };
 
 // Resident warps per SM the register allocation must allow (compile-time
-// tuning knobs): the scan is latency-bound, so occupancy matters; the
-// register-resident top-k needs more registers per thread.
-#ifndef KNN_TARGET_WARPS_SMEM_TOPK
-#define KNN_TARGET_WARPS_SMEM_TOPK 32
+// tuning knobs): the scan is latency-bound, so occupancy matters; rows of
+// more than 8 floats keep the query in registers and get the lower target.
+#ifndef KNN_TARGET_WARPS
+#define KNN_TARGET_WARPS 32
 #endif
-#ifndef KNN_TARGET_WARPS_REG_TOPK
-#define KNN_TARGET_WARPS_REG_TOPK 16
+#ifndef KNN_TARGET_WARPS_WIDE
+#define KNN_TARGET_WARPS_WIDE 16
 #endif
 // Load a small member row together with its band distance (before the band
 // test) so both loads are in flight at once.
@@ -463,34 +515,25 @@ struct QueryRow<0, IDXROW> {
 #define KNN_WALK_OUTWARD 0
 #endif
 
-// Largest list length kept in registers (longer lists live in shared memory).
-#ifndef KNN_REG_TOPK_MAX_L
-#define KNN_REG_TOPK_MAX_L 32
-#endif
-
-// Top-k for lists longer than the register limit: radix-select set
-// (KNN_TOPK_SELECT=1) or sorted shared-memory list with bitonic merges.
-#ifndef KNN_TOPK_SELECT
-#define KNN_TOPK_SELECT 1
+// Largest k kept in a register list (one key per lane): up to 24, so that
+// 8 of the 32 slots or more hold the FP32 band behind the k-th; larger k use
+// the shared-memory candidate set.
+#ifndef KNN_REG_TOPK_MAX_K
+#define KNN_REG_TOPK_MAX_K 24
 #endif
 
 template <int L>
-using TopKFor = std::conditional_t<
-    (L <= KNN_REG_TOPK_MAX_L), RegTopK<L / 32>,
-    std::conditional_t<(KNN_TOPK_SELECT != 0), SelectTopK<L>, SmemTopK<L>>>;
+using TopKFor = std::conditional_t<(L <= 32), RegTopK<L / 32>, SelectTopK<L>>;
 
 // Rows of more than 8 floats keep 4+ float4 of the query in registers: those
 // kernels get the lower occupancy target instead of spilling.
-template <int DP4, int L, int WARPS>
+template <int DP4, int WARPS>
 constexpr int scan_min_blocks() {
-  return (((L <= KNN_REG_TOPK_MAX_L && L > 32) || DP4 == 0 || DP4 >= 4)
-              ? KNN_TARGET_WARPS_REG_TOPK
-              : KNN_TARGET_WARPS_SMEM_TOPK) /
-         WARPS;
+  return ((DP4 == 0 || DP4 >= 4) ? KNN_TARGET_WARPS_WIDE : KNN_TARGET_WARPS) / WARPS;
 }
 
 template <int DP4, bool IDXROW, int L, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, L, WARPS>()))
+__global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
     scan_kernel(const ScanArgs a) {
   using TK = TopKFor<L>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -502,14 +545,15 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, L, WARPS>())
   TK tk;
   tk.init(keys_base + (size_t)w * TK::kSmemKeys);
   tk.k = a.k;
+  tk.d = a.d;
   const float tol = bound_tol(a.d);
-  unsigned evals = 0, visited = 0, pruned = 0;
+  unsigned evals = 0, visited = 0, pruned = 0, checked = 0;
   // small rows: load the member row together with its band distance
   constexpr bool kEagerRow = KNN_EAGER_ROWS && (DP4 > 0 && DP4 <= 2);
   // statistics: per-lane 32-bit counts folded once per query into per-block
   // shared counters, added to the global ones at exit
-  __shared__ unsigned long long blk_ctr[5];
-  if (threadIdx.x < 5) blk_ctr[threadIdx.x] = 0;
+  __shared__ unsigned long long blk_ctr[kScanCounters];
+  if (threadIdx.x < kScanCounters) blk_ctr[threadIdx.x] = 0;
   __syncthreads();
 
   for (;;) {
@@ -700,8 +744,7 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, L, WARPS>())
       }
     }
     tk.finish(lane);
-    tk.write_out(a.out_idx + q * a.k, a.out_dist + q * a.k, a.squared,
-                 a.qc_ref_base ? (int32_t)a.qc_ref_base[qc] : 0, lane);
+    checked += emit_query(tk, a, (int32_t)slot, q, qc, lane);
     if (a.counters) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
@@ -715,13 +758,15 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, L, WARPS>())
         atomicAdd(&blk_ctr[2], (unsigned long long)pruned);
         atomicAdd(&blk_ctr[3], (unsigned long long)tk.pushed);
         atomicAdd(&blk_ctr[4], (unsigned long long)tk.merges);
+        atomicAdd(&blk_ctr[5], (unsigned long long)checked);
       }
     }
-    evals = visited = pruned = 0;
+    evals = visited = pruned = checked = 0;
     tk.pushed = tk.merges = 0;
   }
   __syncthreads();
-  if (a.counters && threadIdx.x < 5) atomicAdd(a.counters + threadIdx.x, blk_ctr[threadIdx.x]);
+  if (a.counters && threadIdx.x < kScanCounters)
+    atomicAdd(a.counters + threadIdx.x, blk_ctr[threadIdx.x]);
 }
 
 template <int DP4, bool IDXROW, int L, int WARPS>
@@ -747,7 +792,7 @@ static int launch_scan_t(const ScanArgs &a, int num_sms, cudaStream_t s) {
 
 template <int DP4, bool IDXROW>
 static int launch_scan_l(const ScanArgs &a, int num_sms, cudaStream_t s) {
-  if (a.k <= 32) return launch_scan_t<DP4, IDXROW, 32, 8>(a, num_sms, s);
+  if (a.k <= KNN_REG_TOPK_MAX_K) return launch_scan_t<DP4, IDXROW, 32, 8>(a, num_sms, s);
   if (a.k <= 64) return launch_scan_t<DP4, IDXROW, 64, 8>(a, num_sms, s);
   if (a.k <= 128) return launch_scan_t<DP4, IDXROW, 128, 8>(a, num_sms, s);
   if (a.k <= 256) return launch_scan_t<DP4, IDXROW, 256, 8>(a, num_sms, s);
@@ -788,11 +833,19 @@ struct ThreadTopK {
 
 // 4 blocks per SM (64 registers; 71 unbounded gave 3): C4 79.3 -> 76.5 ms.
 // Loading member p + 1 while member p is evaluated measured slower.
+//
+// FP64 boundary: the pruning bound is band_hi of the K-th key, so every point
+// inside the final k-th's FP32 band is evaluated; one that does not fit the
+// list sets `lost`.  A query whose band reaches behind its k-th (a key inside
+// it was lost, or the list holds one after the k-th) goes to the band kernel,
+// which re-decides the band in FP64; on data without near-ties at the k-th
+// that is a small fraction of the queries, and FP64 code stays out of this
+// register-bound kernel.
 template <int DP4, bool IDXROW, int K>
 __global__ void __launch_bounds__(256, 4)
     thread_scan_kernel(const ScanArgs a) {
-  __shared__ unsigned long long blk_ctr[5];
-  if (threadIdx.x < 5) blk_ctr[threadIdx.x] = 0;
+  __shared__ unsigned long long blk_ctr[kScanCounters];
+  if (threadIdx.x < kScanCounters) blk_ctr[threadIdx.x] = 0;
   __syncthreads();
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t nslots = a.slot_list ? (int64_t)*a.slot_count : a.m;
@@ -801,12 +854,14 @@ __global__ void __launch_bounds__(256, 4)
     const int64_t slot = a.slot_list ? (int64_t)a.slot_list[t] : t;
     const int64_t q = a.qorder[slot];
     const int qc = a.slot_cl[slot];
-    const float tol = bound_tol(a.d);
+    const int d = a.d;
+    const float tol = bound_tol(d);
     QueryRow<DP4, IDXROW> qr;
     qr.load(a.qrows, q, DP4, nullptr);
     ThreadTopK<K> tk;
     tk.reset();
     float theta = a.theta0[qc];
+    float lost = __int_as_float(0x7f800000);
     // admits every d^2 <= theta0^2, whatever the index
     const uint64_t thr0 = ((uint64_t)__float_as_uint(theta * theta) << 32) | 0xffffffffull;
     const int nr = a.rlen[qc];
@@ -844,14 +899,42 @@ __global__ void __launch_bounds__(256, 4)
         evals++;
         if (!IDXROW) idx = a.sidx[start + p];
         const uint64_t key = make_key(v, idx);
-        if (key < thr0 && key < tk.key[K - 1]) {
-          tk.insert(key);
-          pushed++;
-          if (tk.key[K - 1] != kKeyMax) {
-            theta = sqrtf(key_d2(tk.key[K - 1]));
-            slack = tol * (2.0f * D + 2.0f * theta);
+        if (key < thr0) {
+          if (key < tk.key[K - 1]) {
+            lost = fminf(lost, key_d2(tk.key[K - 1]));  // NaN (empty) is ignored
+            tk.insert(key);
+            pushed++;
+            if (tk.key[K - 1] != kKeyMax) {
+              theta = sqrtf(band_hi(key_d2(tk.key[K - 1]), d));
+              slack = tol * (2.0f * D + 2.0f * theta);
+            }
+          } else {
+            lost = fminf(lost, v);
           }
         }
+      }
+    }
+    // the k-th key, the key behind it, and the FP32 band around the k-th
+    // (selected by masks: a compare-and-select on the runtime k turns the
+    // list into an indexed local-memory array)
+    uint64_t kth = 0, next = 0;
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+      kth |= tk.key[j] & (0ull - (uint64_t)(j == a.k - 1));
+      next |= tk.key[j] & (0ull - (uint64_t)(j == a.k));
+    }
+    if (a.k >= K) next = kKeyMax;
+    bool defer = false;
+    int nlo = 0;
+    const float Dk = key_d2(kth);
+    if (kth != kKeyMax) {
+      const float hi = band_hi(Dk, d);
+      // a band key was dropped, or one sits behind the k-th (NaN: none)
+      defer = lost <= hi || key_d2(next) <= hi;
+      if (defer) {
+        const float lo = band_lo(Dk, d);
+#pragma unroll
+        for (int j = 0; j < K; j++) nlo += key_d2(tk.key[j]) < lo;
       }
     }
     int32_t *oi = a.out_idx + q * a.k;
@@ -866,6 +949,13 @@ __global__ void __launch_bounds__(256, 4)
         const float d2 = key_d2(key);
         od[j] = none ? __int_as_float(0x7f800000) : (a.squared ? d2 : sqrtf(d2));
       }
+    }
+    if (defer) {
+      // the band kernel settles the boundary: it reads the number of keys
+      // below the band and the k-th value from the last slot
+      oi[a.k - 1] = nlo;
+      od[a.k - 1] = Dk;
+      a.unres_slot[atomicAdd(a.unres_count, 1u)] = (int32_t)slot;
     }
   }
   if (a.counters) {
@@ -883,7 +973,7 @@ __global__ void __launch_bounds__(256, 4)
       atomicAdd(&blk_ctr[3], (unsigned long long)pushed);
     }
     __syncthreads();
-    if (threadIdx.x < 5) atomicAdd(a.counters + threadIdx.x, blk_ctr[threadIdx.x]);
+    if (threadIdx.x < kScanCounters) atomicAdd(a.counters + threadIdx.x, blk_ctr[threadIdx.x]);
   }
 }
 
@@ -903,12 +993,209 @@ static int launch_thread_scan(const ScanArgs &a, cudaStream_t s) {
   return go(thread_scan_kernel<DP4, IDXROW, 32>);
 }
 
+// ---------------------------------------------------------------------------
+// Band kernel: the k-th boundary of the queries the scan kernels could not
+// settle (a key of the final band was dropped for lack of room, or the
+// thread scan's list holds one behind the k-th).  One block per query, over
+// the same candidate list: every point whose FP32 d^2 -- computed with the
+// scan's own arithmetic, so the values are the same -- lies inside the band
+// band_lo(Dk) .. band_hi(Dk) of the k-th is found again, and the band's
+// need = k - nlo best by (FP64 d^2, index) are kept in a shared-memory set
+// that is sorted and cut back to `need` whenever it fills, so any number of
+// ties fits.  They are written, in FP32 key order, behind the nlo keys below
+// the band that the scan already wrote.  The scan left nlo and Dk in the
+// query's last output slot.
+// ---------------------------------------------------------------------------
+constexpr int kBandThreads = 128;
+constexpr int kBandCap = 2048;  // >= KNN_MAX_K + kBandThreads: room after a cut
+
+struct BandEntry {
+  unsigned long long d64;  // FP64 d^2 bits (non-negative: they order like the values)
+  unsigned long long key;  // FP32 (d^2, index) key
+};
+
+__device__ __forceinline__ bool band_entry_less(const BandEntry &x, const BandEntry &y) {
+  return x.d64 < y.d64 || (x.d64 == y.d64 && (uint32_t)x.key < (uint32_t)y.key);
+}
+
+// Ascending bitonic sort of e[0..P) (P a power of two) by the block, by
+// (FP64 d^2, index) or by the FP32 key.
+template <bool BY_KEY>
+__device__ void band_sort(BandEntry *e, int P) {
+  for (int size = 2; size <= P; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int t = threadIdx.x; t < (P >> 1); t += blockDim.x) {
+        const int i = 2 * t - (t & (stride - 1));
+        const int j = i + stride;
+        const bool up = (i & size) == 0;
+        const BandEntry x = e[i], y = e[j];
+        const bool gt = BY_KEY ? x.key > y.key : band_entry_less(y, x);
+        if (gt == up) {
+          e[i] = y;
+          e[j] = x;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Cuts the set e[0..*cnt) back to its `need` smallest by (FP64 d^2, index);
+// *thr becomes the need-th (the admission bound) once that many are in.
+__device__ void band_cut(BandEntry *e, int *cnt, BandEntry *thr, int need) {
+  const int c = *cnt;  // read by every thread before the barrier below
+  int P = 1;
+  while (P < c) P <<= 1;
+  for (int i = c + threadIdx.x; i < P; i += blockDim.x) e[i] = BandEntry{~0ull, ~0ull};
+  __syncthreads();
+  band_sort<false>(e, P);
+  if (threadIdx.x == 0) {
+    const int kept = c < need ? c : need;
+    *cnt = kept;
+    if (kept == need) *thr = e[need - 1];
+  }
+  __syncthreads();
+}
+
+// FP32 squared distance over the first d coordinates, dimension order, fma:
+// the scan kernels' value for the same pair (their padded coordinates add
+// exact zeros).
+__device__ __forceinline__ float band_dist2(const float *__restrict__ q,
+                                            const float *__restrict__ r, int d) {
+  float acc = 0.0f;
+  for (int c = 0; c < d; c++) {
+    const float t = __fsub_rn(q[c], r[c]);
+    acc = __fmaf_rn(t, t, acc);
+  }
+  return acc;
+}
+
+__global__ void __launch_bounds__(kBandThreads) band_resolve_kernel(const ScanArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BandEntry *ent = reinterpret_cast<BandEntry *>(smem_raw);
+  float *qv = reinterpret_cast<float *>(ent + kBandCap);  // 4 * dp4 floats
+  __shared__ int s_cnt;
+  __shared__ BandEntry s_thr;
+  const int tid = threadIdx.x, k = a.k, d = a.d, dp4 = a.dp4;
+  const float tol = bound_tol(d);
+  const unsigned total = *a.unres_count;
+  unsigned long long evals = 0;
+  for (unsigned u = blockIdx.x; u < total; u += gridDim.x) {
+    const int32_t slot = a.unres_slot[u];
+    const int64_t q = a.qorder[slot];
+    const int qc = a.slot_cl[slot];
+    int32_t *oi = a.out_idx + q * k;
+    float *od = a.out_dist + q * k;
+    __syncthreads();  // the previous query is done with the shared state
+    const int nlo = oi[k - 1];
+    const float Dk = od[k - 1];
+    const int need = k - nlo;
+    const float lo = band_lo(Dk, d), hi = band_hi(Dk, d), th = sqrtf(hi);
+    for (int c = tid; c < 4 * dp4; c += kBandThreads)
+      qv[c] = reinterpret_cast<const float *>(a.qrows + q * dp4)[c];
+    if (tid == 0) {
+      s_cnt = 0;
+      s_thr = BandEntry{~0ull, ~0ull};
+    }
+    __syncthreads();
+    const int nr = a.rlen[qc];
+    const int32_t *rl = a.rlist + (a.rl_base ? a.rl_base[qc] : (int64_t)qc * a.Rs);
+    for (int j = 0; j < nr; j++) {  // block-uniform
+      const int c = rl[j];
+      const float D =
+          sqrtf(band_dist2(qv, reinterpret_cast<const float *>(a.sreps + (int64_t)c * dp4), d));
+      const float slack = tol * (2.0f * D + 2.0f * th);
+      if (D - a.cmax[c] > th + slack || D + th + slack < a.cmin[c]) continue;
+      const int start = a.soff[c], n_c = a.soff[c + 1] - start;
+      const float lo_e = D - th - slack, hi_e = D + th + slack;
+      int p0 = 0, p1 = n_c;  // first member with d(s, Rc) >= lo_e
+      while (p0 < p1) {
+        const int md = (p0 + p1) >> 1;
+        if (a.sdist[start + md] < lo_e) p0 = md + 1;
+        else p1 = md;
+      }
+      for (int c0 = p0; c0 < n_c; c0 += kBandThreads) {  // block-uniform
+        const int p = c0 + tid;
+        bool past = p >= n_c;
+        if (!past) {
+          const int64_t gp = (int64_t)start + p;
+          if (a.sdist[gp] > hi_e) {
+            past = true;
+          } else {
+            const float v =
+                band_dist2(qv, reinterpret_cast<const float *>(a.srows + gp * dp4), d);
+            if (v >= lo && v <= hi) {
+              const int32_t id = a.sidx[gp];
+              const double w =
+                  dist2_f64(qv, reinterpret_cast<const float *>(a.rrows + (int64_t)id * dp4), d);
+              evals++;
+              const BandEntry e{(unsigned long long)__double_as_longlong(w), make_key(v, id)};
+              if (band_entry_less(e, s_thr)) ent[atomicAdd(&s_cnt, 1)] = e;
+            }
+          }
+        }
+        const int any_past = __syncthreads_or(past);
+        if (s_cnt > kBandCap - kBandThreads) band_cut(ent, &s_cnt, &s_thr, need);
+        if (any_past) break;
+      }
+    }
+    band_cut(ent, &s_cnt, &s_thr, need);
+    // the band's share of the result, in FP32 key order
+    const int got = s_cnt;  // == need: the scan's own band keys are all found again
+    int P = 1;
+    while (P < got) P <<= 1;
+    for (int i = got + tid; i < P; i += kBandThreads) ent[i] = BandEntry{~0ull, ~0ull};
+    __syncthreads();
+    band_sort<true>(ent, P);
+    const int32_t base = a.qc_ref_base ? (int32_t)a.qc_ref_base[qc] : 0;
+    for (int t = tid; t < need; t += kBandThreads) {
+      const uint64_t key = t < got ? ent[t].key : kKeyMax;
+      const bool none = key == kKeyMax;
+      oi[nlo + t] = none ? -1 : key_idx(key) - base;
+      od[nlo + t] =
+          none ? __int_as_float(0x7f800000) : (a.squared ? key_d2(key) : sqrtf(key_d2(key)));
+    }
+  }
+  if (a.counters) {
+    for (int o = 16; o > 0; o >>= 1) evals += __shfl_xor_sync(kFull, evals, o);
+    if ((tid & 31) == 0 && evals) atomicAdd(a.counters + 5, evals);
+    if (blockIdx.x == 0 && tid == 0) atomicAdd(a.counters + 6, (unsigned long long)total);
+  }
+}
+
+static int launch_band_resolve(const ScanArgs &a, int num_sms, cudaStream_t s) {
+  const size_t smem = kBandCap * sizeof(BandEntry) + (size_t)a.dp4 * sizeof(float4);
+  if (smem > 48 * 1024)
+    KNN_CUDA_TRY(cudaFuncSetAttribute(band_resolve_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // a persistent grid over the list, whose length only the device knows
+  // (an empty list costs one launch that returns at once)
+  band_resolve_kernel<<<2 * num_sms, kBandThreads, smem, s>>>(a);
+  KNN_LAUNCH_CHECK();
+  return KNN_OK;
+}
+
 #ifndef KNN_THREAD_SCAN_MAX_K
 #define KNN_THREAD_SCAN_MAX_K 32
 #endif
 
+static int launch_scan_kernels(const ScanArgs &a, int num_sms, cudaStream_t s);
+
+// The scan of one batch of query slots, then the band kernel for the queries
+// whose k-th boundary the scan left open.
 int launch_scan(const ScanArgs &a, int num_sms, cudaStream_t s) {
   if (a.m == 0) return KNN_OK;
+  if (!a.rrows || !a.unres_slot || !a.unres_count) {
+    set_error("scan: the FP64 boundary buffers are missing");
+    return KNN_EINTERNAL;
+  }
+  KNN_CUDA_TRY(cudaMemsetAsync(a.unres_count, 0, sizeof(unsigned), s));
+  const int rc = launch_scan_kernels(a, num_sms, s);
+  if (rc != KNN_OK) return rc;
+  return launch_band_resolve(a, num_sms, s);
+}
+
+static int launch_scan_kernels(const ScanArgs &a, int num_sms, cudaStream_t s) {
   // thread per query: small k, rows of at most 8 floats, and short bands (at
   // most 128 points per cluster on average).  Measured: 4,096 surface clouds
   // (~70-100 points per cluster, k = 16) 143 -> 67 ms; a dense 3-D set with

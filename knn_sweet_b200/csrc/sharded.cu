@@ -165,7 +165,7 @@ extern "C" int knn_join_sharded(const float *q, int64_t m, const float *r, int64
       st->dist_evals += s.st.dist_evals;
       st->clusters_visited += s.st.clusters_visited;
       st->clusters_pruned += s.st.clusters_pruned;
-      st->refine_rechecks += s.st.refine_rechecks;
+      st->fp64_rechecks += s.st.fp64_rechecks;
       st->topk_candidates += s.st.topk_candidates;
       st->topk_merges += s.st.topk_merges;
       st->ms_build = s.st.ms_build > st->ms_build ? s.st.ms_build : st->ms_build;
@@ -175,6 +175,7 @@ extern "C" int knn_join_sharded(const float *q, int64_t m, const float *r, int64
       st->sreps_used = s.st.sreps_used;
       st->kernels_launched += s.st.kernels_launched;
       st->refine_fallbacks += s.st.refine_fallbacks;
+      st->band_queries += s.st.band_queries;
     }
     st->pairs_total = m * n;
     st->pairs_pruned = st->pairs_total - st->dist_evals;

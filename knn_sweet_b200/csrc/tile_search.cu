@@ -243,16 +243,6 @@ __device__ __forceinline__ float dist2_cols(const float4 *__restrict__ q,
   return acc;
 }
 
-__device__ __forceinline__ double dist2_cols_f64(const float *__restrict__ q,
-                                                 const float *__restrict__ r, int d) {
-  double acc = 0.0;
-  for (int c = 0; c < d; c++) {
-    const double t = (double)q[c] - (double)r[c];
-    acc = fma(t, t, acc);
-  }
-  return acc;
-}
-
 // Sorts the n <= 32E keys s[0..n) ascending in registers (padding with the
 // largest key) and writes 32E sorted keys back to s.  One warp.
 template <int E>
@@ -268,11 +258,6 @@ __device__ __forceinline__ void sort_keys_in_registers(uint64_t *s, int n, int l
 #pragma unroll
   for (int j = 0; j < E; j++) s[E * lane + j] = x[j];
   __syncwarp();
-}
-
-// FP32 rounding band of a squared distance D computed by dist2_cols.
-__device__ __forceinline__ float band_eps(float D, int d) {
-  return (float)(d + 4) * 5.9604645e-8f * D;
 }
 
 __global__ void __launch_bounds__(kTM)
@@ -684,7 +669,7 @@ __global__ void __launch_bounds__(kTM)
         sorted = true;
         if (m1 > k) {
           const float Dk = key_d2(keys[k - 1]);
-          const float lim2 = Dk + 2.0f * band_eps(Dk, d);
+          const float lim2 = band_hi(Dk, d);
           int w = 0;
           for (int b0 = 0; b0 < m1; b0 += 32) {
             const int e = b0 + lane;
@@ -695,7 +680,7 @@ __global__ void __launch_bounds__(kTM)
       } else if (!fb && m1 > k) {
         const uint64_t kth = warp_select_kth(keys, m1, k, whist, lane);
         const float Dk = key_d2(kth);
-        const float lim2 = Dk + 2.0f * band_eps(Dk, d);
+        const float lim2 = band_hi(Dk, d);
         int w = 0;
         for (int b0 = 0; b0 < m1; b0 += 32) {
           const int e = b0 + lane;
@@ -722,7 +707,7 @@ __global__ void __launch_bounds__(kTM)
           // keys at or above Dk - band were ranked in FP32 only to within
           // rounding: order them again by (FP64 d^2, index)
           const float Dk = key_d2(keys[k - 1]);
-          const float lo_v = Dk - 2.0f * band_eps(Dk, d);
+          const float lo_v = band_lo(Dk, d);
           int lo = 0;
           for (int b0 = 0; b0 < m2; b0 += 32) {
             const int e = b0 + lane;
@@ -736,7 +721,7 @@ __global__ void __launch_bounds__(kTM)
             uint64_t *perm = keys + np2;
             for (int e = lane; e < bsz; e += 32) {
               const int32_t id = key_idx(keys[lo + e]);
-              d64[e] = dist2_cols_f64(
+              d64[e] = dist2_f64(
                   qf, reinterpret_cast<const float *>(a.rrows + (size_t)id * dp4), d);
             }
             __syncwarp();

@@ -30,7 +30,7 @@ class JoinStats:
     pairs_pruned: int
     clusters_visited: int
     clusters_pruned: int
-    refine_rechecks: int
+    fp64_rechecks: int
     topk_candidates: int
     topk_merges: int
     ms_build: float
@@ -40,6 +40,7 @@ class JoinStats:
     sreps_used: int
     kernels_launched: int
     refine_fallbacks: int = 0
+    band_queries: int = 0
 
 
 def _options(qreps, sreps, seed, rep_trials, precision, margin,
@@ -77,8 +78,10 @@ def knnjoin(queries, sources=None, k: int = 200, *, qreps: int = 0, sreps: int =
 
     queries: (m, d) float32; sources: (n, d) float32 or None for a self-join
     (the reference's sample run joins a set with itself, run_sample.sh:1).
-    Returns (idx int32 (m, k), dist float32 (m, k)) ascending by distance,
-    ties to the lower source row; slots beyond n hold (-1, inf).  With
+    Returns (idx int32 (m, k), dist float32 (m, k)): per query the k nearest
+    by (FP64 squared distance, source row) -- the FP64 brute-force join's set,
+    ties to the lower source row -- ascending by FP32 distance; slots beyond n
+    hold (-1, inf).  With
     stats=True a JoinStats is returned as a third element.  `out` may give
     preallocated (idx, dist) arrays of the input's kind (e.g. pinned host
     memory for the host path).  squared=True returns squared distances;

@@ -60,7 +60,7 @@ def test_default_options():
     o = _lib.default_options()
     assert (o.qreps, o.sreps, o.seed, o.rep_trials, o.precision, o.margin, o.flags) == \
         (0, 0, 2015, 10, _lib.KNN_FP32, 32, 0)
-    assert _lib.load().knn_abi_version() == 1
+    assert _lib.load().knn_abi_version() == 2
 
 
 def _call_join(q, r, d, k, opt=None, m=None, n=None):

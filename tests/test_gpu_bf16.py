@@ -41,7 +41,6 @@ def test_float_data_sets_match_fp64_oracle(cuda_device, oracle, d, k):
     oi, od = oracle.bruteforce_f64(q, r, k)
     assert np.array_equal(_sets(idx), _sets(oi))
     np.testing.assert_allclose(dist, od, rtol=1e-5, atol=1e-6)
-    assert (idx == oi).all(axis=1).mean() > 0.99
     assert 0 <= st.refine_fallbacks <= q.shape[0]
 
 

@@ -1,38 +1,18 @@
 """GPU parity tests of the plain FP32 pruned join against the FP64 oracle.
 
-Bar: identical neighbour index lists under the (distance, lower index) order;
-FP32 distances within 1e-5 relative of the FP64 oracle (bit-exact on integer
-data, where every FP32 squared distance is an exact integer).  On float data
-an index may differ from the oracle only where the oracle's own distances
-tie within 1e-5 relative (FP32 rounding can order such a pair either way).
+Bar (tests/parity.py): per query the neighbour index set equals the FP64
+join's exactly (ties at equal distance to the lower index), FP32 distances
+within 1e-5 relative; on integer data, where every FP32 squared distance is an
+exact integer, identical lists and bit-identical distances.
 """
 import numpy as np
 import pytest
 
 from knn_sweet_b200 import data, knnjoin
 from tests.golden.make_golden import load_cases
+from tests.parity import assert_matches
 
 pytestmark = pytest.mark.gpu
-
-REL = 1e-5
-
-
-def assert_matches(idx, dist, oi, od, exact: bool):
-    idx = np.asarray(idx)
-    dist = np.asarray(dist)
-    if exact:
-        assert np.array_equal(idx, oi)
-        assert np.array_equal(dist, od.astype(np.float32))
-        return
-    fin = np.isfinite(od)
-    assert np.array_equal(np.isfinite(dist), fin)
-    np.testing.assert_allclose(dist[fin], od[fin], rtol=REL, atol=0)
-    bad = np.argwhere(idx != oi)
-    for i, j in bad:
-        # only a near-tie in the oracle may swap
-        v = od[i, j]
-        near = np.abs(od[i] - v) <= REL * max(v, 1e-30)
-        assert near.sum() >= 2, (i, j, idx[i, j], oi[i, j])
 
 
 def torch_join(q, r, k, **kw):
