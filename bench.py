@@ -48,7 +48,9 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-forms", action="store_true",
-                    help="skip the BF16+refine and batched form comparisons")
+                    help="skip the precision, d=32, batching and differentiation forms")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip the run of the reference's own CUDA program")
     return ap.parse_args(argv)
 
 
@@ -289,6 +291,7 @@ def run_ours(args):
         scans.append(st.ms_search)
         evals.append(st.dist_evals)
         launches.append(st.kernels_launched)
+    boundary = {"fp64_rechecks": st.fp64_rechecks, "band_queries": st.band_queries}
     scan_ms = statistics.mean(scans)
     build_ms = statistics.mean(builds)
 
@@ -320,11 +323,13 @@ def run_ours(args):
     peak, peak_kind = measured_peaks()
     bytes_per_query = 4 * D * 2 + 8 * K  # 4d(1 + N/M) + 8k, self-join N = M
     achieved = bytes_per_query * m / (scan_ms * 1e-3) / 1e9
-    traffic = None
+    traffic, warp_inst = None, None
     tp = ROOT / "profiles" / "scan_skin_selfjoin_traffic.json"
     if tp.exists():
         try:
-            traffic = json.loads(tp.read_text()).get("dram_bytes_per_launch")
+            prof = json.loads(tp.read_text())
+            traffic = prof.get("dram_bytes_per_launch")
+            warp_inst = prof.get("warp_inst_per_launch")
         except Exception:
             traffic = None
     fp32_flops = statistics.mean(evals) * 3 * D
@@ -339,7 +344,8 @@ def run_ours(args):
                    "l2": "flushed (256 MB write) before every timed step",
                    "build_ms": build_ms, "scan_ms": scan_ms,
                    "dist_evals_per_query": statistics.mean(evals) / m,
-                   "pairs_pruned_frac": 1.0 - statistics.mean(evals) / (m * m)},
+                   "pairs_pruned_frac": 1.0 - statistics.mean(evals) / (m * m),
+                   "k_th_boundary": boundary},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "kernel": "scan_kernel", "peak_source": peak_kind,
@@ -348,10 +354,32 @@ def run_ours(args):
         "gpu_launches": int(statistics.mean(launches)) * args.steps,
         "clocks": sampler.summary(),
     }
+    # the bound the scan kernel has: instruction issue.  Warp instructions per
+    # launch (one ncu capture of the same launch) over its event-timed
+    # duration, against SMs x 4 schedulers x one instruction per clock at the
+    # median SM clock of the timed region
+    clk = line["clocks"].get("sm_mhz") or line["clocks"].get("sm_max_mhz")
+    if warp_inst and clk:
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        ach = warp_inst / (scan_ms * 1e-3) / 1e12
+        pk = sms * 4 * clk * 1e6 / 1e12
+        line["roofline"]["issue"] = {
+            "achieved": ach, "peak": pk, "unit": "T warp-instructions/s", "frac": ach / pk,
+            "warp_inst_per_launch": warp_inst,
+            "warp_inst_per_eval": warp_inst / statistics.mean(evals),
+            "peak_source": f"{sms} SMs x 4 issue slots x {clk:.0f} MHz (median under load)"}
     if e2e:
         line["e2e"] = e2e
+    # the headline join against the FP64 oracle on a sample of queries
+    hi, hd = step()
+    torch.cuda.synchronize(dev)
+    line["oracle_err"] = oracle_err(hi.cpu().numpy(), hd.cpu().numpy(), x, x, K,
+                                    _sample_rows(m, 2000, 5))
+    del hi, hd
     if world == 1 and not args.no_forms:
         line["forms"] = run_forms(torch, dev, flush)
+    if world == 1 and not args.no_reference_cuda:
+        line["reference_cuda"] = reference_cuda(x)
     if world == 1 and not args.no_cpu_baseline:
         cores = host_cores()
         sample = cpu_sample_size(x, cores, 10.0)
@@ -382,24 +410,52 @@ def _time_steps(torch, dev, fn, steps, flush):
     return statistics.mean(ms)
 
 
-def run_forms(torch, dev, flush, steps=3):
-    """The precision and batching forms beside the plain FP32 join.
+# ----------------------------------------------------------------------------
+# checks against the FP64 brute-force oracle (after the timed regions; the
+# oracle is the checker, never timed)
+# ----------------------------------------------------------------------------
+def oracle_err(idx, dist, q, r, k, rows, squared=False):
+    """Error of a join's rows against the FP64 oracle: the fraction of sampled
+    queries whose neighbour set differs, and the largest relative distance
+    error (position by position)."""
+    from oracle import oracle as orc
+    oi, od = orc.bruteforce_f64(q, r, k, qrows=np.asarray(rows, np.int64), threads=host_cores())
+    return compare_to_oracle(np.asarray(idx)[rows], np.asarray(dist)[rows], oi, od, squared)
 
-    precision: 2,000,000 reference / 200,000 query points, d=128, k=100
-    (seeded mixture of 4,096 Gaussians), plain FP32 vs BF16+refine on the same
-    representatives; neighbour-set agreement between the two forms.
-    batching: 4,096 ellipsoid clouds of 256..16,384 points, d=3, per-cloud
-    self-join k=16: one graph-replayed batched call vs one plain call per cloud.
-    """
+
+def compare_to_oracle(idx, dist, oi, od, squared=False):
+    idx = np.asarray(idx)
+    dist = np.asarray(dist, np.float64)
+    if squared:
+        dist = np.sqrt(dist)
+    sets = (np.sort(idx, 1) != np.sort(oi, 1)).any(1)
+    fin = np.isfinite(od)
+    both = np.array_equal(np.isfinite(dist), fin)
+    rel = np.abs(dist[fin] - od[fin]) / np.maximum(od[fin], 1e-30)
+    return {"queries": int(idx.shape[0]), "set_mismatch_frac": float(sets.mean()),
+            "max_rel_dist_err": float(rel.max()) if rel.size else 0.0,
+            "missing_slots_agree": bool(both)}
+
+
+def _merge_errs(errs, what):
+    n = sum(e["queries"] for e in errs)
+    return {"sample": what, "queries": n,
+            "set_mismatch_frac": sum(e["set_mismatch_frac"] * e["queries"] for e in errs)
+            / max(1, n),
+            "max_rel_dist_err": max(e["max_rel_dist_err"] for e in errs),
+            "missing_slots_agree": all(e["missing_slots_agree"] for e in errs)}
+
+
+def _sample_rows(m, count, seed):
+    return np.sort(np.random.default_rng(seed).choice(m, min(count, m), replace=False))
+
+
+def _pair_forms(torch, dev, flush, r, q, k, kw, steps, sample, seed):
+    """Plain FP32 and BF16+refine on the same inputs and representatives: time,
+    statistics, agreement of the two forms and each form's oracle error."""
     import knn_sweet_b200 as ks
-    from knn_sweet_b200 import data
-    from knn_sweet_b200.batched import BatchedJoinGraph
-    out = {}
-    r, q = data.config3()
     rt, qt = torch.from_numpy(r).to(dev), torch.from_numpy(q).to(dev)
-    del r, q
-    m, k = qt.shape[0], 100
-    kw = dict(qreps=8192, sreps=8192, lloyd_iters=4)
+    m = qt.shape[0]
     res, forms = {}, {}
     for prec in ("fp32", "bf16_refine"):
         o = (torch.empty((m, k), dtype=torch.int32, device=dev),
@@ -411,17 +467,60 @@ def run_forms(torch, dev, flush, steps=3):
         forms[prec] = {"queries_per_s": m / (ms * 1e-3), "ms_per_step": ms,
                        "build_ms": st.ms_build, "search_ms": st.ms_search,
                        "dist_evals_per_query": st.dist_evals / m,
-                       "fp64_rechecks": st.fp64_rechecks,
+                       "fp64_rechecks": st.fp64_rechecks, "band_queries": st.band_queries,
                        "fallback_queries": st.refine_fallbacks}
     a, b = res["fp32"][0], res["bf16_refine"][0]
     same = (torch.sort(a, 1)[0] == torch.sort(b, 1)[0]).all(1).float().mean().item()
-    out["precision"] = {
-        "workload": f"N=2,000,000 M={m} d=128 k={k} reps 8192/8192 lloyd 4, synthetic "
-                    "4,096-Gaussian mixture", "fp32": forms["fp32"],
-        "bf16_refine": forms["bf16_refine"], "same_neighbor_sets": same,
-        "bf16_over_fp32": forms["bf16_refine"]["queries_per_s"] / forms["fp32"]["queries_per_s"]}
-    del rt, qt, res, a, b
+    torch.cuda.synchronize(dev)
+    del rt, qt
+    rows = _sample_rows(m, sample, seed)
+    from oracle import oracle as orc
+    oi, od = orc.bruteforce_f64(q, r, k, qrows=rows.astype(np.int64), threads=host_cores())
+    for prec in forms:
+        forms[prec]["oracle_err"] = compare_to_oracle(res[prec][0][rows].cpu().numpy(),
+                                                      res[prec][1][rows].cpu().numpy(), oi, od)
+    return forms, same
 
+
+def form_precision(torch, dev, flush, steps):
+    """Precision form (2,000,000 reference / 200,000 query points, d=128,
+    k=100, seeded mixture of 4,096 Gaussians): plain FP32 vs BF16+refine on the
+    same representatives."""
+    from knn_sweet_b200 import data
+    r, q = data.config3()
+    k = 100
+    forms, same = _pair_forms(torch, dev, flush, r, q, k,
+                              dict(qreps=8192, sreps=8192, lloyd_iters=4), steps, 500, 33)
+    return {"workload": f"N={r.shape[0]} M={q.shape[0]} d=128 k={k} reps 8192/8192 lloyd 4, "
+                        "synthetic 4,096-Gaussian mixture",
+            "fp32": forms["fp32"], "bf16_refine": forms["bf16_refine"],
+            "same_neighbor_sets": same,
+            "bf16_over_fp32": forms["bf16_refine"]["queries_per_s"] / forms["fp32"]["queries_per_s"]}
+
+
+def form_c2(torch, dev, flush, steps):
+    """Higher-dimension plain join (1,000,000 reference / 100,000 query points,
+    d=32, k=32, 1,000 representatives per side, seeded mixture of 1,000
+    Gaussians), both forms."""
+    from knn_sweet_b200 import data
+    r, q = data.config2()
+    k = 32
+    forms, same = _pair_forms(torch, dev, flush, r, q, k,
+                              dict(qreps=1000, sreps=1000, lloyd_iters=3), steps, 1000, 22)
+    return {"workload": f"N={r.shape[0]} M={q.shape[0]} d=32 k={k} reps 1000/1000 lloyd 3, "
+                        "synthetic 1,000-Gaussian mixture",
+            "fp32": forms["fp32"], "bf16_refine": forms["bf16_refine"],
+            "same_neighbor_sets": same,
+            "bf16_over_fp32": forms["bf16_refine"]["queries_per_s"] / forms["fp32"]["queries_per_s"]}
+
+
+def form_batching(torch, dev, flush, steps):
+    """Batching form (4,096 ellipsoid clouds of 256..16,384 points, d=3,
+    per-cloud self-join k=16): one graph-replayed batched call vs one plain call
+    per cloud; oracle error over 16 sampled whole clouds."""
+    import knn_sweet_b200 as ks
+    from knn_sweet_b200 import data
+    from knn_sweet_b200.batched import BatchedJoinGraph
     pts, off = data.ellipsoid_clouds()
     x = torch.from_numpy(pts).to(dev)
     mq, kb = x.shape[0], 16
@@ -439,13 +538,120 @@ def run_forms(torch, dev, flush, steps=3):
             ks.knnjoin(x[a0:a1], None, kb, out=(oi[a0:a1], od[a0:a1]))
     ms_p = _time_steps(torch, dev, per_cloud, 1, flush)
     same_b = (torch.sort(oi, 1)[0] == torch.sort(bi, 1)[0]).all(1).float().mean().item()
-    out["batching"] = {
-        "workload": f"{len(bounds)} ellipsoid clouds, {mq} points, d=3, per-cloud self-join "
-                    f"k={kb}", "batched_graph": {"queries_per_s": mq / (ms_b * 1e-3),
-                                                 "ms_per_step": ms_b},
-        "per_cloud_calls": {"queries_per_s": mq / (ms_p * 1e-3), "ms_per_step": ms_p},
-        "same_neighbor_sets": same_b, "batched_over_per_cloud": ms_p / ms_b}
+    bi, bd = bi.cpu().numpy(), bd.cpu().numpy()
+    from oracle import oracle as orc
+    errs = []
+    for c in _sample_rows(len(bounds), 16, 44):
+        a0, a1 = bounds[c]
+        ci, cd = orc.bruteforce_f64(pts[a0:a1], pts[a0:a1], kb, threads=host_cores())
+        errs.append(compare_to_oracle(bi[a0:a1], bd[a0:a1], ci, cd))
+    return {"workload": f"{len(bounds)} ellipsoid clouds, {mq} points, d=3, per-cloud "
+                        f"self-join k={kb}",
+            "batched_graph": {"queries_per_s": mq / (ms_b * 1e-3), "ms_per_step": ms_b,
+                              "oracle_err": _merge_errs(errs, "16 whole clouds")},
+            "per_cloud_calls": {"queries_per_s": mq / (ms_p * 1e-3), "ms_per_step": ms_p},
+            "same_neighbor_sets": same_b, "batched_over_per_cloud": ms_p / ms_b}
+
+
+def form_differentiation(torch, dev, flush, steps):
+    """Differentiation form (64 blob cloud pairs of 2,048..32,768 points, d=3):
+    forward + hand-written backward of the summed k nearest squared distances in
+    both directions (k=8, and the k=1 Chamfer loss).  Checked on 16 sampled
+    pairs: forward neighbour sets against the FP64 oracle, and the gradient
+    against the FP64 gradient of the same loss over the oracle's pairs."""
+    from knn_sweet_b200 import data
+    from knn_sweet_b200.autograd import knn_chamfer_batched, knn_dist2_batched
+    pairs = data.blob_cloud_pairs()
+    xo = np.concatenate([[0], np.cumsum([len(p[0]) for p in pairs])]).astype(np.int64)
+    yo = np.concatenate([[0], np.cumsum([len(p[1]) for p in pairs])]).astype(np.int64)
+    xs = np.concatenate([p[0] for p in pairs])
+    ys = np.concatenate([p[1] for p in pairs])
+    x = torch.from_numpy(xs).to(dev).requires_grad_(True)
+    y = torch.from_numpy(ys).to(dev).requires_grad_(True)
+    npts = x.shape[0] + y.shape[0]
+    out = {"workload": f"{len(pairs)} blob cloud pairs, {npts} points, d=3, loss = sum of "
+                       "k nearest squared distances in both directions, forward + backward"}
+    for k in (8, 1):
+        def fwd_bwd():
+            x.grad = y.grad = None
+            knn_chamfer_batched(x, xo, y, yo, k).backward()
+        ms = _time_steps(torch, dev, fwd_bwd, steps, flush)
+        out[f"k{k}"] = {"queries_per_s": npts / (ms * 1e-3), "ms_per_step": ms}
+    # checks (k = 8)
+    k = 8
+    x.grad = y.grad = None
+    knn_chamfer_batched(x, xo, y, yo, k).backward()
+    gx, gy = x.grad.double().cpu().numpy(), y.grad.double().cpu().numpy()
+    with torch.no_grad():
+        dxy, ixy = knn_dist2_batched(x.detach(), xo, y.detach(), yo, k)
+        dyx, iyx = knn_dist2_batched(y.detach(), yo, x.detach(), xo, k)
+    ixy, iyx = ixy.cpu().numpy(), iyx.cpu().numpy()
+    dxy, dyx = dxy.cpu().numpy(), dyx.cpu().numpy()
+    from oracle import oracle as orc
+    errs, gerr = [], 0.0
+    for c in _sample_rows(len(pairs), 16, 55):
+        xa, xb, ya, yb = xo[c], xo[c + 1], yo[c], yo[c + 1]
+        px, py = xs[xa:xb].astype(np.float64), ys[ya:yb].astype(np.float64)
+        oxy, dxy_o = orc.bruteforce_f64(xs[xa:xb], ys[ya:yb], k, threads=host_cores())
+        oyx, dyx_o = orc.bruteforce_f64(ys[ya:yb], xs[xa:xb], k, threads=host_cores())
+        errs.append(compare_to_oracle(ixy[xa:xb], dxy[xa:xb], oxy, dxy_o, squared=True))
+        errs.append(compare_to_oracle(iyx[ya:yb], dyx[ya:yb], oyx, dyx_o, squared=True))
+        # FP64 gradient of the pair's loss over the oracle's neighbour pairs
+        rgx, rgy = np.zeros_like(px), np.zeros_like(py)
+        dv = px[:, None, :] - py[oxy]                  # x_i - y_j
+        rgx += 2 * dv.sum(1)
+        np.add.at(rgy, oxy.ravel(), -2 * dv.reshape(-1, 3))
+        dv = py[:, None, :] - px[oyx]                  # y_j - x_i
+        rgy += 2 * dv.sum(1)
+        np.add.at(rgx, oyx.ravel(), -2 * dv.reshape(-1, 3))
+        scale = max(np.abs(rgx).max(), np.abs(rgy).max(), 1e-30)
+        gerr = max(gerr, np.abs(gx[xa:xb] - rgx).max() / scale,
+                   np.abs(gy[ya:yb] - rgy).max() / scale)
+    out["k8"]["oracle_err"] = _merge_errs(errs, "16 pairs, both directions")
+    out["k8"]["grad_max_err_rel_to_max"] = float(gerr)
     return out
+
+
+def run_forms(torch, dev, flush, steps=3):
+    """The precision, batching and differentiation forms beside the plain FP32
+    join, and the d = 32 plain join; each with its error against the FP64
+    oracle."""
+    out = {"precision": form_precision(torch, dev, flush, steps)}
+    torch.cuda.empty_cache()
+    out["c2"] = form_c2(torch, dev, flush, steps)
+    torch.cuda.empty_cache()
+    out["batching"] = form_batching(torch, dev, flush, steps)
+    torch.cuda.empty_cache()
+    out["differentiation"] = form_differentiation(torch, dev, flush, steps)
+    torch.cuda.empty_cache()
+    return out
+
+
+def reference_cuda(x: np.ndarray):
+    """The reference's own CUDA program (oracle/_ref/knnjoin_ref, built from the
+    reference's sources by oracle/build_ref.sh) on the same points written as its
+    text input, reps 800/800, K=200: its own "total time" line
+    (src/knnjoin.cu:1136, which covers knnjoin.cu:274-1135 and so excludes its
+    H2D copies and representative draw) and the wall time of its process."""
+    ref = ROOT / "oracle" / "_ref" / "knnjoin_ref"
+    if not ref.exists():
+        return {"unavailable": "oracle/_ref/knnjoin_ref not built (oracle/build_ref.sh)"}
+    import tempfile
+    from oracle.compare_ref import agreement, run_reference
+    try:
+        with tempfile.TemporaryDirectory() as td:
+            ri, rd, info = run_reference(x, K, REPS, Path(td), timeout=300)
+    except Exception as e:  # reported, not raised: the arm is informational
+        return {"unavailable": f"reference run failed: {str(e)[:200]}"}
+    rows = _sample_rows(x.shape[0], 1000, 12)
+    from oracle import oracle as orc
+    oi, od = orc.bruteforce_f64(x, x, K, qrows=rows.astype(np.int64), threads=host_cores())
+    return {"total_time_ms": info["total_time_s"] * 1e3 if info["total_time_s"] else None,
+            "process_wall_s": info["wall_s"], "dist_evals": info["dist_evals"],
+            "coverage": "its own total time: clustering, bounds, filter and scan of the GPU "
+                        "program (knnjoin.cu:274-1135); excludes its text parsing, H2D copies "
+                        "and representative draw, which this build's step includes",
+            "vs_fp64_oracle": agreement(ri[rows], rd[rows], oi, od)}
 
 
 def main(argv=None):

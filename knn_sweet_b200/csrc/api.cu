@@ -193,6 +193,7 @@ enum CtrSlot {
   kCtrTile,                             // tile-search statistics (4)
   kCtrFallback = kCtrTile + 4,          // slots the tile search leaves to the scan
   kCtrUnres,                            // queries left to the band kernel
+  kCtrInexactQ,                         // the query side is not small integers
   kCtrCount
 };
 
@@ -368,6 +369,7 @@ struct RefSide {
   float4 *srows = nullptr;     // cluster-contiguous rows
   float *sdist = nullptr, *cmin = nullptr, *cmax = nullptr;
   int32_t *sidx = nullptr;
+  int *inexact = nullptr;      // device flag: 0 when the rows are small integers
 };
 
 // Builds the reference side; the arrays it keeps come from `keep`, scratch
@@ -389,6 +391,10 @@ int build_ref_side(Arena &keep, Arena &tmp, const float *r, int64_t n, int d, in
     KNN_TRY(launch_pack_rows(r, n, d, dp4s, p, s));
     R->Rp = p;
   }
+  KNN_TRY(keep.alloc(&R->inexact, 1));
+  KNN_CUDA_TRY(cudaMemsetAsync(R->inexact, 0, sizeof(int), s));
+  KNN_TRY(launch_exact_check(reinterpret_cast<const float *>(R->Rp), n * dp4s * 4, d,
+                             R->inexact, s));
   const bool use_tc = (o.flags & KNN_NO_TENSOR_CORES) == 0;
   KNN_TRY(build_clusters(keep, tmp, R->Rp, n, d, dp4s, Rs, o.seed, o.rep_trials, o.lloyd_iters,
                          use_tc, dev_err, s, &R->sset));
@@ -485,6 +491,7 @@ int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t 
   const bool use_tc = (o.flags & KNN_NO_TENSOR_CORES) == 0;
   const float4 *Qp = nullptr;
   ClusterSet qset;
+  const int *q_inexact = R.inexact;
   if (self_rows) {
     Qp = Rp;
     qset = sset;
@@ -497,6 +504,9 @@ int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t 
       KNN_TRY(launch_pack_rows(q, m, d, dp4s, p, s));
       Qp = p;
     }
+    int *qf = reinterpret_cast<int *>(ctr + kCtrInexactQ);
+    KNN_TRY(launch_exact_check(reinterpret_cast<const float *>(Qp), m * dp4s * 4, d, qf, s));
+    q_inexact = qf;
     KNN_TRY(build_clusters(ar, ar, Qp, m, d, dp4s, Rq, o.seed, o.rep_trials, o.lloyd_iters,
                            use_tc, dev_err, s, &qset));
   }
@@ -596,6 +606,8 @@ int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t 
   a.Rs = Rs;
   a.n_ref = n;
   a.rrows = Rp;
+  a.inexact_r = R.inexact;
+  a.inexact_q = q_inexact;
   a.out_idx = out_idx;
   a.out_dist = out_dist;
   KNN_TRY(ar.alloc(&a.unres_slot, (size_t)m));

@@ -455,7 +455,7 @@ int batched_impl(const float *q, const int64_t *qoff_h, const float *r, const in
     auto body = [&]() -> int {
       // [0] scan work counter, [1 ..] scan statistics, then the count of
       // queries left to the band kernel
-      constexpr int kCtr = 2 + kScanCounters;
+      constexpr int kCtr = 4 + kScanCounters;  // + the two sides' exactness flags
       KNN_TRY(ar.alloc(&ctr, kCtr));
       KNN_CUDA_TRY(cudaMemsetAsync(ctr, 0, kCtr * sizeof(unsigned long long), s));
       if (roff_h[ncloud] == 0) {  // no reference points in any cloud
@@ -557,6 +557,17 @@ int batched_impl(const float *q, const int64_t *qoff_h, const float *r, const in
       a.Rs = S.Rtot;
       a.n_ref = S.total;
       a.rrows = S.rows;
+      {
+        int *fr = reinterpret_cast<int *>(ctr + 2 + kScanCounters);
+        int *fq = reinterpret_cast<int *>(ctr + 3 + kScanCounters);
+        KNN_TRY(launch_exact_check(reinterpret_cast<const float *>(S.rows), n * dp4 * 4, d, fr,
+                                   s));
+        if (!self)
+          KNN_TRY(launch_exact_check(reinterpret_cast<const float *>(Q.rows), m * dp4 * 4, d, fq,
+                                     s));
+        a.inexact_r = fr;
+        a.inexact_q = self ? fr : fq;
+      }
       a.out_idx = out_idx;
       a.out_dist = out_dist;
       KNN_TRY(ar.alloc(&a.unres_slot, (size_t)m));

@@ -547,6 +547,32 @@ static int grid_for(int64_t work, int threads) {
   return (int)(g < 1 ? 1 : g);
 }
 
+// Exactness of FP32 distances: raises *inexact unless every value of x is an
+// integer of magnitude at most `bound`.  With bound = sqrt(2^24 / d) / 2 every
+// coordinate difference, square and partial sum of a squared distance is an
+// integer below 2^24, so the FP32 squared distance is exact, equal to the FP64
+// one, and the two rank every pair alike (the k-th boundary needs no FP64
+// re-check).  The reference's sample data (integer RGB values) is of this
+// kind.
+__global__ void exact_check_kernel(const float *__restrict__ x, int64_t count, float bound,
+                                   int *inexact) {
+  bool bad = false;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const float v = x[t];
+    bad |= !(v == rintf(v) && fabsf(v) <= bound);
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(inexact, 1);
+}
+
+int launch_exact_check(const float *x, int64_t count, int d, int *inexact, cudaStream_t s) {
+  if (count == 0) return KNN_OK;
+  const float bound = floorf(sqrtf(16777216.0f / (float)d) * 0.5f);
+  exact_check_kernel<<<grid_for(count, 256), 256, 0, s>>>(x, count, bound, inexact);
+  KNN_LAUNCH_CHECK();
+  return KNN_OK;
+}
+
 int launch_pack_rows(const float *src, int64_t n, int d, int dp4, float4 *dst,
                      cudaStream_t s) {
   if (n == 0) return KNN_OK;

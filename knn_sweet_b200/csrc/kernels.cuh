@@ -41,6 +41,9 @@ struct ScanArgs {
                             // the mean cluster size the scan variant is chosen by
   const float4 *rrows;      // n x dp4 reference rows, original order (the
                             // FP64 re-check of the k-th boundary)
+  const int *inexact_r;     // device flags of the two sides, 0 when every
+  const int *inexact_q;     // coordinate is a small integer (then FP32
+                            // distances are exact and rank like FP64)
   int32_t *out_idx;         // m x k
   float *out_dist;          // m x k
   int32_t *unres_slot;      // room for every slot of the launch: queries
@@ -52,6 +55,9 @@ struct ScanArgs {
 
 int launch_pack_rows(const float *src, int64_t n, int d, int dp4, float4 *dst,
                      cudaStream_t s);
+// Raises *inexact unless every value of x[0..count) is an integer small enough
+// that FP32 squared distances in dimension d are exact.
+int launch_exact_check(const float *x, int64_t count, int d, int *inexact, cudaStream_t s);
 int launch_rep_select(const float4 *rows, int dp4, const int32_t *cand_dev,
                       int R, int trials, uint32_t *score_dev, float4 *reps,
                       int32_t *rep_rows, cudaStream_t s);

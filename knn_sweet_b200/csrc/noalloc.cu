@@ -101,8 +101,10 @@ struct SideBufs {
 };
 
 // Device counters: [0] scan work counter, [1 ..] scan statistics, then the
-// count of queries left to the band kernel and the device error flag.
-constexpr int kCtrUnres = 1 + kScanCounters, kCtrErr = kCtrUnres + 1, kCtrCount = kCtrErr + 1;
+// count of queries left to the band kernel, the device error flag and the
+// two sides' exactness flags.
+constexpr int kCtrUnres = 1 + kScanCounters, kCtrErr = kCtrUnres + 1;
+constexpr int kCtrInexactR = kCtrErr + 1, kCtrInexactQ = kCtrErr + 2, kCtrCount = kCtrErr + 3;
 
 struct Plan {
   int64_t m = 0, n = 0;
@@ -347,6 +349,16 @@ int noalloc_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d
   a.Rs = p.Rs;
   a.n_ref = n;
   a.rrows = Rp;
+  {
+    int *fr = reinterpret_cast<int *>(p.ctr + kCtrInexactR);
+    int *fq = reinterpret_cast<int *>(p.ctr + kCtrInexactQ);
+    rc = launch_exact_check(reinterpret_cast<const float *>(Rp), n * p.dp4s * 4, d, fr, s);
+    if (rc == KNN_OK && !p.share)
+      rc = launch_exact_check(reinterpret_cast<const float *>(Qp), m * p.dp4s * 4, d, fq, s);
+    if (rc != KNN_OK) return rc;
+    a.inexact_r = fr;
+    a.inexact_q = p.share ? fr : fq;
+  }
   a.out_idx = out_idx;
   a.out_dist = out_dist;
   a.unres_slot = p.unres;

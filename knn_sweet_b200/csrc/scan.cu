@@ -334,6 +334,12 @@ __device__ __forceinline__ void topk_push(TK &tk, uint64_t key, int lane) {
   tk.pushed += cnt;
 }
 
+// Whether every FP32 squared distance of the join is exact (both sides hold
+// small integers), so that FP32 keys rank exactly like FP64 ones.
+__device__ __forceinline__ bool fp32_exact(const ScanArgs &a) {
+  return a.inexact_r && a.inexact_q && (*a.inexact_r | *a.inexact_q) == 0;
+}
+
 // FP64 re-decision of one query's k-th boundary, by one warp.  s[0..n) holds
 // the query's candidate keys sorted ascending, n > k; s[0..nlo) lie below the
 // FP32 band of the k-th (band_lo(Dk) .. band_hi(Dk)), s[nlo..nhi) inside it,
@@ -385,13 +391,13 @@ __device__ __noinline__ void band_resolve_fp64(uint64_t *s, int nlo, int nhi, in
 }
 
 // End of one query of the warp scan: sorts the candidates, settles the k-th
-// boundary in FP64 (or, when a key of its band was dropped for lack of room,
+// boundary in FP64 unless the join's FP32 distances are exact (or, when a key of its band was dropped for lack of room,
 // hands the query to the band kernel: the last output slot then carries the
 // number of keys below the band and the FP32 k-th value), writes the k
 // results.  Returns the FP64 distances evaluated.
 template <class TK>
 __device__ __forceinline__ unsigned emit_query(TK &tk, const ScanArgs &a, int32_t slot, int64_t q,
-                                               int qc, int lane) {
+                                               int qc, bool exact32, int lane) {
   const int n = tk.sorted(lane);
   uint64_t *s = tk.buf;
   const int k = a.k;
@@ -399,7 +405,7 @@ __device__ __forceinline__ unsigned emit_query(TK &tk, const ScanArgs &a, int32_
   int nlo = 0;
   float Dk = 0.0f;
   unsigned checked = 0;
-  if (n >= k) {
+  if (n >= k && !exact32) {  // exact FP32 distances: the (d^2, index) order is FP64's
     Dk = key_d2(s[k - 1]);
     const float lo = band_lo(Dk, a.d), hi = band_hi(Dk, a.d);
     int nhi = 0;
@@ -546,6 +552,7 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
   tk.init(keys_base + (size_t)w * TK::kSmemKeys);
   tk.k = a.k;
   tk.d = a.d;
+  const bool exact32 = fp32_exact(a);
   const float tol = bound_tol(a.d);
   unsigned evals = 0, visited = 0, pruned = 0, checked = 0;
   // small rows: load the member row together with its band distance
@@ -744,7 +751,7 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
       }
     }
     tk.finish(lane);
-    checked += emit_query(tk, a, (int32_t)slot, q, qc, lane);
+    checked += emit_query(tk, a, (int32_t)slot, q, qc, exact32, lane);
     if (a.counters) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
@@ -927,7 +934,7 @@ __global__ void __launch_bounds__(256, 4)
     bool defer = false;
     int nlo = 0;
     const float Dk = key_d2(kth);
-    if (kth != kKeyMax) {
+    if (kth != kKeyMax && !fp32_exact(a)) {
       const float hi = band_hi(Dk, d);
       // a band key was dropped, or one sits behind the k-th (NaN: none)
       defer = lost <= hi || key_d2(next) <= hi;

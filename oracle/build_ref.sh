@@ -3,7 +3,8 @@
 # into oracle/_ref/ (git-ignored; travels to the GPU machine with the tree):
 #   oracle/_ref/knnjoin_ref   the reference's knnjoin (src/knnjoin.cu)
 #   oracle/_ref/ref_shim.so   the LD_PRELOAD interposer of oracle/ref_shim.c
-# Usage: oracle/build_ref.sh [reference-root]   (default /root/reference)
+# Usage: oracle/build_ref.sh REFERENCE_ROOT   (or KNN_REFERENCE_ROOT in the
+# environment): the root of a checkout of the reference (src/, include/).
 #
 # The sources are compiled from a temporary copy outside this repository with
 # two changes (below): getPoint (include/common8.h:27) is
@@ -13,7 +14,11 @@
 # Makefile (-w -std=c++11 -O3 -fopenmp -lcublas) with sm_100a for sm_35 and
 # the CUDA runtime linked dynamically so that ref_shim.so can interpose.
 set -euo pipefail
-REF=${1:-/root/reference}
+REF=${1:-${KNN_REFERENCE_ROOT:-}}
+if [ -z "$REF" ]; then
+  echo "usage: $0 REFERENCE_ROOT (or set KNN_REFERENCE_ROOT)" >&2
+  exit 2
+fi
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 mkdir -p "$OUT"

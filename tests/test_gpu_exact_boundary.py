@@ -68,11 +68,26 @@ def test_band_larger_than_the_band_kernel_buffer(cuda_device, oracle):
 
 
 def test_integer_ties_unchanged(cuda_device, oracle):
-    # on integer data FP32 is exact: ties at the k-th keep the lower indices
+    # small integers: every FP32 squared distance is exact, the join detects it
+    # and needs no FP64 step; ties at the k-th keep the lower indices
     rng = np.random.default_rng(3)
     x = rng.integers(0, 6, size=(12000, 3)).astype(np.float32)
     for k in (10, 50, 300):
-        idx, dist = knnjoin(x, None, k)
+        idx, dist, st = knnjoin(x, None, k, stats=True)
         rows = np.arange(0, 12000, 61)
         oi, od = oracle.bruteforce_f64(x, x, k, qrows=rows)
         assert_matches(idx[rows], dist[rows], oi, od, exact=True)
+        assert st.fp64_rechecks == 0 and st.band_queries == 0
+
+
+def test_large_integers_take_the_fp64_step(cuda_device, oracle):
+    # integers too large for exact FP32 squared distances (2^12 apart in 3-D
+    # already exceed 2^24): the FP64 step runs and the sets stay the oracle's
+    rng = np.random.default_rng(4)
+    r = (rng.integers(0, 3, size=(20000, 3)) * 40000 + rng.integers(0, 9, size=(20000, 3)))
+    r = r.astype(np.float32)
+    q = r[rng.choice(20000, 300, replace=False)] + 1.0
+    idx, dist, st = knnjoin(q, r, 40, stats=True)
+    oi, od = oracle.bruteforce_f64(q, r, 40)
+    assert_matches(idx, dist, oi, od)
+    assert st.fp64_rechecks + st.band_queries > 0
