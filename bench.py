@@ -12,8 +12,12 @@ write) before every timed step, outside the timed events.
     python bench.py [--gpus N --steps K --warmup W]        # this build
     python bench.py --impl reference ...                    # CPU reference arm
 
-Multi-GPU (torchrun): every rank joins its own point set (seed 1 + rank), no
-data-path collective ("weak" scaling); the step time is the max over ranks.
+Multi-GPU (torchrun, one process per GPU): ONE join split across the ranks
+("strong" scaling).  Every rank builds the same index from the same points
+(the build is deterministic), takes its share of the query clusters --
+balanced by estimated work, knn_join_partition_device -- and the result rows
+are all-gathered to rank 0 (NCCL) inside the step; the step time is the max
+over ranks.
 """
 from __future__ import annotations
 
@@ -73,9 +77,51 @@ def max_over_ranks(pg, value: float, device) -> float:
 
 
 def weak_scaling_value(world: int, points_per_rank: int, ms_per_step: float) -> float:
-    """Whole-job queries/s: every rank joins its own set of points_per_rank
+    """Whole-job queries/s when every rank joins its own set of points_per_rank
     queries; the step time is the slowest rank's."""
     return world * points_per_rank / (ms_per_step * 1e-3)
+
+
+def strong_scaling_value(queries: int, ms_per_step: float) -> float:
+    """Whole-job queries/s of one join of `queries` queries split across the
+    ranks; the step time is the slowest rank's."""
+    return queries / (ms_per_step * 1e-3)
+
+
+def gather_rows(pg, rows, ri, rd, m: int, k: int, device):
+    """Rank 0 receives the full (m, k) result of a partitioned join: every rank
+    contributes its query rows and their (k) indices and distances, padded to
+    the largest part and all-gathered (NCCL between GPUs, gloo on CPU).
+    Returns (idx, dist) on rank 0, None on the other ranks; every rank takes
+    the same collective steps."""
+    import torch
+    cnt = torch.tensor([rows.numel()], dtype=torch.int64, device=device)
+    pg.all_reduce(cnt, op=pg.ReduceOp.MAX)
+    mx = int(cnt.item())
+    n = rows.numel()
+    pr = torch.full((mx,), -1, dtype=torch.int32, device=device)
+    pi = torch.full((mx, k), -1, dtype=torch.int32, device=device)
+    pd = torch.zeros((mx, k), dtype=torch.float32, device=device)
+    pr[:n] = rows
+    pi[:n] = ri
+    pd[:n] = rd
+    world = pg.get_world_size()
+    lr = [torch.empty_like(pr) for _ in range(world)]
+    li = [torch.empty_like(pi) for _ in range(world)]
+    ld = [torch.empty_like(pd) for _ in range(world)]
+    pg.all_gather(lr, pr)
+    pg.all_gather(li, pi)
+    pg.all_gather(ld, pd)
+    if pg.get_rank() != 0:
+        return None
+    out_i = torch.empty((m, k), dtype=torch.int32, device=device)
+    out_d = torch.empty((m, k), dtype=torch.float32, device=device)
+    for g in range(world):
+        ok = lr[g] >= 0
+        sel = lr[g][ok].long()
+        out_i[sel] = li[g][ok]
+        out_d[sel] = ld[g][ok]
+    return out_i, out_d
 
 
 def measured_peaks():
@@ -214,7 +260,7 @@ def run_reference(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
         "config": {"workload": f"skin-like self-join N=M={m} d=3 k={K} reps {REPS}/{REPS}",
                    "reference_arm": "CPU restatement of the reference's pruned join "
@@ -247,14 +293,23 @@ def run_ours(args):
                                  device_id=dev)
         pg = tdist
 
-    x = data.skin_like(args.n, seed=1 + rank)
+    x = data.skin_like(args.n, seed=1)
     m = x.shape[0]
     xt = torch.from_numpy(x).to(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 
     def step(stats=False):
-        return ks.knnjoin(xt, None, K, qreps=REPS, sreps=REPS, stats=stats)
+        if world == 1:
+            return ks.knnjoin(xt, None, K, qreps=REPS, sreps=REPS, stats=stats)
+        # this rank's part of the one join, then the rows to rank 0
+        out = ks.knnjoin_partition(xt, None, K, part=rank, nparts=world, qreps=REPS,
+                                   sreps=REPS, stats=stats)
+        idx, dist, rows = out[:3]
+        rl = rows.long()
+        got = gather_rows(pg, rows, idx[rl], dist[rl], m, K, dev)
+        res = got if got is not None else (idx, dist)
+        return (*res, out[3]) if stats else res
 
     for _ in range(args.warmup):
         step()
@@ -279,7 +334,7 @@ def run_ours(args):
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = max_over_ranks(pg, sum(step_ms), dev)
     ms_per_step = total_ms / args.steps
-    value = weak_scaling_value(world, m, ms_per_step)
+    value = strong_scaling_value(m, ms_per_step)
 
     # same steps with the library's own stage events (build / scan split),
     # giving the scan kernel's duration for the roofline
@@ -296,9 +351,35 @@ def run_ours(args):
     build_ms = statistics.mean(builds)
 
     # end to end through the public API with host buffers (pinned), copies
-    # inside every step
+    # inside every step (several ranks: the inputs copied in on every rank,
+    # the gathered result copied out on rank 0)
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and world > 1:
+        qh = torch.from_numpy(x).pin_memory()
+        oi = torch.empty((m, K), dtype=torch.int32).pin_memory()
+        od = torch.empty((m, K), dtype=torch.float32).pin_memory()
+        wall = []
+        for i in range(max(3, args.steps // 3) + 1):
+            flush.fill_(i & 0xFF)
+            torch.cuda.synchronize(dev)
+            pg.barrier()
+            t0 = time.perf_counter()
+            xd = qh.to(dev, non_blocking=True)
+            idx, dist, rows = ks.knnjoin_partition(xd, None, K, part=rank, nparts=world,
+                                                   qreps=REPS, sreps=REPS)
+            rl = rows.long()
+            got = gather_rows(pg, rows, idx[rl], dist[rl], m, K, dev)
+            if got is not None:
+                oi.copy_(got[0], non_blocking=True)
+                od.copy_(got[1], non_blocking=True)
+            torch.cuda.synchronize(dev)
+            if i > 0:
+                wall.append(time.perf_counter() - t0)
+        e2e_s = max_over_ranks(pg, statistics.mean(wall), dev)
+        e2e = {"value": strong_scaling_value(m, e2e_s * 1e3), "unit": "queries/s",
+               "h2d_bytes_per_step": int(x.nbytes) * world, "d2h_bytes_per_step": int(m * K * 8),
+               "ms_per_step": e2e_s * 1e3}
+    if not args.no_e2e and world == 1:
         qh = torch.from_numpy(x).pin_memory().numpy()
         oi = torch.empty((m, K), dtype=torch.int32).pin_memory().numpy()
         od = torch.empty((m, K), dtype=torch.float32).pin_memory().numpy()
@@ -311,9 +392,21 @@ def run_ours(args):
             ks.knnjoin(qh, None, K, qreps=REPS, sreps=REPS, out=(oi, od))
             wall.append(time.perf_counter() - t0)
         e2e_s = max_over_ranks(pg, statistics.mean(wall), dev)
-        e2e = {"value": weak_scaling_value(world, m, e2e_s * 1e3), "unit": "queries/s",
+        e2e = {"value": strong_scaling_value(m, e2e_s * 1e3), "unit": "queries/s",
                "h2d_bytes_per_step": int(x.nbytes), "d2h_bytes_per_step": int(m * K * 8),
                "ms_per_step": e2e_s * 1e3}
+
+    # the headline join against the FP64 oracle on a sample of queries (every
+    # rank joins its part; rank 0 holds the gathered result)
+    hi, hd = step()[:2]
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        # the parts' statistics: evaluations summed, stage times the slowest
+        tot = torch.tensor([statistics.mean(evals)], dtype=torch.float64, device=dev)
+        pg.all_reduce(tot, op=pg.ReduceOp.SUM)
+        evals = [float(tot.item())]
+        scan_ms = max_over_ranks(pg, scan_ms, dev)
+        build_ms = max_over_ranks(pg, build_ms, dev)
 
     if rank != 0:
         if pg:
@@ -336,11 +429,12 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "fp32",
         "data": "synthetic: seeded 2-Gaussian integer RGB mixture standing in for the "
                 "Skin Segmentation table",
         "config": {"workload": f"skin-like self-join N=M={m} d=3 k={K} reps {REPS}/{REPS}",
-                   "form": "plain FP32 pruned join", "parallelism": f"replicas x{world}",
+                   "form": "plain FP32 pruned join", "parallelism": (f"query-cluster partition x{world}, results all-gathered to rank 0"
+                                   if world > 1 else "one GPU"),
                    "l2": "flushed (256 MB write) before every timed step",
                    "build_ms": build_ms, "scan_ms": scan_ms,
                    "dist_evals_per_query": statistics.mean(evals) / m,
@@ -370,9 +464,6 @@ def run_ours(args):
             "peak_source": f"{sms} SMs x 4 issue slots x {clk:.0f} MHz (median under load)"}
     if e2e:
         line["e2e"] = e2e
-    # the headline join against the FP64 oracle on a sample of queries
-    hi, hd = step()
-    torch.cuda.synchronize(dev)
     line["oracle_err"] = oracle_err(hi.cpu().numpy(), hd.cpu().numpy(), x, x, K,
                                     _sample_rows(m, 2000, 5))
     del hi, hd

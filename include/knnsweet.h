@@ -227,6 +227,19 @@ int knn_join_batched_device(const float *q, const int64_t *q_offsets,
                             void *stream);
 
 /*
+ * knn_join_batched_device on HOST buffers: q, r, out_idx and out_dist are host
+ * memory (the reference keeps its inputs and result in host arrays,
+ * src/knnjoin.cu:1003-1033, and runs one pair of point sets per process).  The
+ * clouds are copied to the current device on a stream of the call's own,
+ * joined, and the result copied back; the call returns when it is complete.
+ * Offsets, limits, options and results as for knn_join_batched_device.
+ */
+int knn_join_batched(const float *q, const int64_t *q_offsets, const float *r,
+                     const int64_t *r_offsets, int32_t ncloud, int32_t d, int32_t k,
+                     int32_t *out_idx, float *out_dist, const knn_options *opt,
+                     knn_stats *st);
+
+/*
  * Reusable index of a reference set.  The reference rebuilds everything on
  * every run (clusterReps, src/knnjoin.cu:166-411), although its source side --
  * representatives, assignment, sorted member lists (knnjoin.cu:223-240,
@@ -251,23 +264,42 @@ int knn_index_free(knn_index *index);
 int knn_index_info(const knn_index *index, int64_t *n, int32_t *d, int32_t *reps);
 
 /*
- * knn_join over several GPUs of this process, by query ranges.  No
- * counterpart in the reference, which runs on one GPU (its whole join,
- * src/knnjoin.cu:983-1172, is what every shard does for its queries).
- * Host buffers as in knn_join.  The m queries are split into ndev contiguous
- * ranges as even as the count allows; shard i runs on devices[i] (an id may
- * repeat: its shards then run concurrently on separate streams) in a host
- * thread of its own, copies in the n references and its queries, builds the
- * reference index there (the same options and seed on every device, so the
- * same index) and joins its queries, writing rows [q0, q0 + m_i) of out_idx /
- * out_dist.  No data crosses between GPUs.  The result is knn_join's.  stats
- * (optional): counts summed over the shards, times the slowest shard's
- * (ms_build includes its index build), qreps_used summed.  Errors: the first
- * failing shard's code, its message prefixed with the shard and device.
+ * knn_join over several GPUs of this process.  No counterpart in the
+ * reference, which runs its search on one GPU (src/knnjoin.cu:1103-1129).
+ * Host buffers as in knn_join.  The reference index and the query clusters
+ * are built once, on devices[0]; the query clusters are split into ndev
+ * contiguous ranges balanced by their estimated work (query count times the
+ * band sizes they can scan), so no query cluster is split; every other listed
+ * device receives a peer copy of what the search reads and searches its range,
+ * storing its results into devices[0]'s result buffer through peer memory
+ * (into a local buffer merged on devices[0] where peer access is missing).
+ * An id may repeat: its shards then run concurrently on separate streams.
+ * The result is knn_join's.  stats (optional): counts summed over the shards,
+ * ms_build the build on devices[0], ms_search the slowest shard (peer copies
+ * included).  Errors: the first failing call's code and message.
  */
 int knn_join_sharded(const float *q, int64_t m, const float *r, int64_t n, int32_t d,
                      int32_t k, int32_t *out_idx, float *out_dist, const knn_options *opt,
                      const int32_t *devices, int32_t ndev, knn_stats *stats);
+
+/*
+ * One part of a join split across processes (one process per GPU, e.g. under
+ * torchrun): every process calls it with the same inputs and options on its
+ * own device and stream, part = its rank, nparts = the number of processes.
+ * Each builds the same index (the build is deterministic), computes the same
+ * partition of the query clusters as knn_join_sharded and searches only part
+ * `part`: the result rows of those queries are written into out_idx /
+ * out_dist (device, m x k; other rows are left untouched), their query row
+ * ids into out_rows[0 .. *out_count) (device, room for m; may be NULL), and
+ * *out_count (host) is set.  Synchronises the stream once (to plan the
+ * partition).  The parts of all processes together are knn_join's result.
+ * No reference counterpart.
+ */
+int knn_join_partition_device(const float *q, int64_t m, const float *r, int64_t n,
+                              int32_t d, int32_t k, int32_t part, int32_t nparts,
+                              int32_t *out_idx, float *out_dist, int32_t *out_rows,
+                              int64_t *out_count, const knn_options *opt, knn_stats *st,
+                              void *stream);
 
 /*
  * Returns the device scratch memory the library keeps cached between calls

@@ -91,6 +91,12 @@ SIGNATURES = {
     "knn_join_batched_device": (_c_int, [_vp, _vp, _vp, _vp, _c_i32, _c_i32, _c_i32, _vp, _vp,
                                          ctypes.POINTER(KnnOptions),
                                          ctypes.POINTER(KnnStats), _vp]),
+    "knn_join_partition_device": (_c_int, [_vp, _c_i64, _vp, _c_i64, _c_i32, _c_i32, _c_i32,
+                                           _c_i32, _vp, _vp, _vp, ctypes.POINTER(_c_i64),
+                                           ctypes.POINTER(KnnOptions),
+                                           ctypes.POINTER(KnnStats), _vp]),
+    "knn_join_batched": (_c_int, [_vp, _vp, _vp, _vp, _c_i32, _c_i32, _c_i32, _vp, _vp,
+                                  ctypes.POINTER(KnnOptions), ctypes.POINTER(KnnStats)]),
     "knn_join_sharded": (_c_int, [_vp, _c_i64, _vp, _c_i64, _c_i32, _c_i32, _vp, _vp,
                                   ctypes.POINTER(KnnOptions), _vp, _c_i32,
                                   ctypes.POINTER(KnnStats)]),

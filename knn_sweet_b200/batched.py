@@ -51,8 +51,9 @@ def knnjoin_batched(queries, q_offsets, sources=None, r_offsets=None, k: int = 1
                     squared: bool = False, stats: bool = False, out=None):
     """k nearest neighbours of every query among its own cloud's points.
 
-    queries: (M, d) float32 CUDA tensor (numpy arrays are copied to the current
-    device and the result copied back); q_offsets: ncloud + 1 host offsets.
+    queries: (M, d) float32 CUDA tensor (joined by knn_join_batched_device on
+    the current stream) or host array (joined by knn_join_batched, which copies
+    in and out itself); q_offsets: ncloud + 1 host offsets.
     sources / r_offsets: the reference clouds, or None for a per-cloud
     self-join.  Returns (idx int32 (M, k), dist float32 (M, k)), indices
     relative to each cloud's first reference row, ascending by distance, ties
@@ -69,9 +70,8 @@ def knnjoin_batched(queries, q_offsets, sources=None, r_offsets=None, k: int = 1
         raise ValueError("q_offsets and r_offsets must describe the same number of clouds")
     host = not (isinstance(queries, torch.Tensor) and queries.is_cuda)
     if host:
-        q = torch.as_tensor(np.ascontiguousarray(queries, dtype=np.float32)).cuda()
-        r = q if sources is None else torch.as_tensor(
-            np.ascontiguousarray(sources, dtype=np.float32)).cuda()
+        return _knnjoin_batched_host(lib, queries, qo, sources, ro, k, seed, rep_trials,
+                                     autotune, squared, stats, out)
     else:
         q = queries.detach().contiguous()
         r = q if sources is None else sources.detach().contiguous()
@@ -103,6 +103,39 @@ def knnjoin_batched(queries, q_offsets, sources=None, r_offsets=None, k: int = 1
     _lib.check(rc)
     if host:
         idx, dist = idx.cpu().numpy(), dist.cpu().numpy()
+    if stats:
+        return idx, dist, JoinStats(**st.as_dict())
+    return idx, dist
+
+
+def _knnjoin_batched_host(lib, queries, qo, sources, ro, k, seed, rep_trials, autotune,
+                          squared, stats, out):
+    q = np.ascontiguousarray(queries, dtype=np.float32)
+    r = q if sources is None else np.ascontiguousarray(sources, dtype=np.float32)
+    if q.ndim != 2 or r.ndim != 2 or r.shape[1] != q.shape[1]:
+        raise ValueError("queries and sources must be 2-D float32 with the same d")
+    M, d = q.shape
+    if qo[-1] != M or ro[-1] != r.shape[0]:
+        raise ValueError("the last offset must equal the number of rows")
+    if out is not None:
+        idx, dist = out
+        if (idx.shape != (M, k) or dist.shape != (M, k) or idx.dtype != np.int32
+                or dist.dtype != np.float32 or not idx.flags.c_contiguous
+                or not dist.flags.c_contiguous):
+            raise ValueError("out must be C-contiguous (M, k) int32 / float32 arrays")
+    else:
+        idx = np.empty((M, k), np.int32)
+        dist = np.empty((M, k), np.float32)
+    opt = _batched_options(seed, rep_trials, autotune, squared)
+    st = _lib.KnnStats()
+    rc = lib.knn_join_batched(q.ctypes.data_as(ctypes.c_void_p),
+                              qo.ctypes.data_as(ctypes.c_void_p),
+                              r.ctypes.data_as(ctypes.c_void_p),
+                              ro.ctypes.data_as(ctypes.c_void_p), qo.size - 1, d, k,
+                              idx.ctypes.data_as(ctypes.c_void_p),
+                              dist.ctypes.data_as(ctypes.c_void_p), ctypes.byref(opt),
+                              ctypes.byref(st) if stats else None)
+    _lib.check(rc)
     if stats:
         return idx, dist, JoinStats(**st.as_dict())
     return idx, dist

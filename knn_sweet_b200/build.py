@@ -35,7 +35,7 @@ NVCC_FLAGS = ARCH + [
 CU_SOURCES = ["api.cu", "build_index.cu", "scan.cu", "backward.cu", "noalloc.cu", "assign_tc.cu", "batched.cu",
               "tile_search.cu", "sharded.cu"]
 HEADERS = ["common.cuh", "kernels.cuh", "glibc_rand.h", "tc_common.cuh", "bounds.cuh",
-           "warp_select.cuh"]
+           "warp_select.cuh", "pipeline.cuh"]
 
 
 def nvcc() -> str:

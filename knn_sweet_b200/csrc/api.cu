@@ -24,6 +24,7 @@
 #include "common.cuh"
 #include "glibc_rand.h"
 #include "kernels.cuh"
+#include "pipeline.cuh"
 
 namespace knnsweet {
 
@@ -131,71 +132,7 @@ int check_options(const knn_options *opt, knn_options *o) {
   return KNN_OK;
 }
 
-namespace {
 
-// Stream-ordered scratch: every allocation is released on the same stream
-// when the arena goes out of scope.
-class Arena {
- public:
-  explicit Arena(cudaStream_t s) : s_(s) {}
-  ~Arena() {
-    for (void *p : ptrs_) cudaFreeAsync(p, s_);
-  }
-  Arena(const Arena &) = delete;
-  Arena &operator=(const Arena &) = delete;
-
-  // Hands the allocations made so far to the caller: they outlive the arena.
-  std::vector<void *> take() {
-    std::vector<void *> out;
-    out.swap(ptrs_);
-    return out;
-  }
-
-  template <class T>
-  int alloc(T **out, size_t count) {
-    *out = nullptr;
-    if (count == 0) count = 1;
-    if (!pool_) {
-      int rc = scratch_pool(&pool_);
-      if (rc != KNN_OK) return rc;
-    }
-    void *p = nullptr;
-    cudaError_t e = cudaMallocFromPoolAsync(&p, count * sizeof(T), pool_, s_);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      set_error("device allocation of %zu bytes failed: %s", count * sizeof(T),
-                cudaGetErrorString(e));
-      return e == cudaErrorMemoryAllocation ? KNN_ENOMEM : KNN_ECUDA;
-    }
-    ptrs_.push_back(p);
-    *out = static_cast<T *>(p);
-    return KNN_OK;
-  }
-
- private:
-  cudaStream_t s_;
-  cudaMemPool_t pool_ = nullptr;
-  std::vector<void *> ptrs_;
-};
-
-#define KNN_TRY(expr)        \
-  do {                       \
-    int rc_ = (expr);        \
-    if (rc_ != KNN_OK) return rc_; \
-  } while (0)
-
-// Device counters of one call, zeroed at its start.
-enum CtrSlot {
-  kCtrWork = 0,                         // scan work counter
-  kCtrScan = 1,                         // the scan statistics (kScanCounters)
-  kCtrErr = kCtrScan + kScanCounters,   // device error flag (bounded waits)
-  kCtrTileWork,                         // tile-search tile counter
-  kCtrTile,                             // tile-search statistics (4)
-  kCtrFallback = kCtrTile + 4,          // slots the tile search leaves to the scan
-  kCtrUnres,                            // queries left to the band kernel
-  kCtrInexactQ,                         // the query side is not small integers
-  kCtrCount
-};
 
 __global__ void fill_empty_kernel(int32_t *idx, float *dist, int64_t count) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
@@ -238,15 +175,6 @@ int default_reps(int64_t n) {
   return (int)r;
 }
 
-// One clustered point set.
-struct ClusterSet {
-  int R = 0;
-  float4 *reps = nullptr;     // R x dp4s
-  int32_t *rep_rows = nullptr;
-  uint64_t *skeys = nullptr;  // n sorted (cluster, distance) keys
-  int32_t *perm = nullptr;    // sorted position -> input row
-  int32_t *off = nullptr;     // R + 1
-};
 
 int build_clusters(Arena &keep, Arena &ar, const float4 *rows, int64_t n, int d, int dp4s, int R,
                    uint32_t seed, int trials, int lloyd_iters, bool use_tc, int *err,
@@ -323,16 +251,6 @@ struct EventSet {
   }
 };
 
-// Host destination of the result for the host-buffer entry point: the scan
-// then runs in row chunks and each chunk's rows are copied back on `copy`
-// while the next chunk is computed.  `done` tells whether the copies were
-// enqueued (otherwise the caller copies the whole result).
-struct HostSink {
-  int32_t *idx;
-  float *dist;
-  cudaStream_t copy;
-  bool done;
-};
 
 // Events of the chunked copies, destroyed once both streams are idle.
 struct ChunkEvents {
@@ -357,20 +275,6 @@ void row_geometry(int d, int *dp4s, int *tmpl) {
   }
 }
 
-// The reference side of a join: representatives, clusters, the
-// cluster-contiguous rows and their bounds.  Depends only on the reference
-// set and the options that shape its clusters.
-struct RefSide {
-  int64_t n = 0;
-  int d = 0, dp4s = 0, tmpl = 0, Rs = 0;
-  bool idx_in_row = false;
-  ClusterSet sset;
-  const float4 *Rp = nullptr;  // packed rows, original order
-  float4 *srows = nullptr;     // cluster-contiguous rows
-  float *sdist = nullptr, *cmin = nullptr, *cmax = nullptr;
-  int32_t *sidx = nullptr;
-  int *inexact = nullptr;      // device flag: 0 when the rows are small integers
-};
 
 // Builds the reference side; the arrays it keeps come from `keep`, scratch
 // from `tmp`.  With copy_rows the packed rows are always a copy (an index
@@ -467,62 +371,63 @@ int join_device_impl(const float *q, int64_t m, const float *r, int64_t n,
   return query_impl(R, share, q, m, k, out_idx, out_dist, o, st, s, sink, ar, evs, ctr);
 }
 
-// The query side of a join against a built reference side.  `ctr`
-// (kCtrCount counters, zeroed) and the events come from the caller; event 0 is recorded.
-int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t k,
-               int32_t *out_idx, float *out_dist, const knn_options &o, knn_stats *st,
-               cudaStream_t s, HostSink *sink, Arena &ar, EventSet &evs,
-               unsigned long long *ctr) {
-  const int64_t n = R.n;
-  const int d = R.d, dp4s = R.dp4s, tmpl = R.tmpl, Rs = R.Rs;
-  const bool idx_in_row = R.idx_in_row;
-  const ClusterSet &sset = R.sset;
-  const float4 *Rp = R.Rp;
-  float4 *srows = R.srows;
-  float *sdist = R.sdist, *cmin = R.cmin, *cmax = R.cmax;
-  int32_t *sidx = R.sidx;
-  if (st) st->pairs_total = m * n;
-  int dev = 0, num_sms = 148;
-  KNN_CUDA_TRY(cudaGetDevice(&dev));
-  KNN_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
-  const bool self_rows = share;
+
+int build_query_side(const RefSide &R, bool share, const float *q, int64_t m, int32_t k,
+                     const knn_options &o, Arena &ar, unsigned long long *ctr, cudaStream_t s,
+                     QuerySide *Q) {
+  const int d = R.d, dp4s = R.dp4s, Rs = R.Rs;
   const int Rq = share ? Rs : query_rep_count(o, m, d, k, false, Rs);
   int *dev_err = reinterpret_cast<int *>(ctr + kCtrErr);
   const bool use_tc = (o.flags & KNN_NO_TENSOR_CORES) == 0;
-  const float4 *Qp = nullptr;
-  ClusterSet qset;
-  const int *q_inexact = R.inexact;
-  if (self_rows) {
-    Qp = Rp;
-    qset = sset;
+  Q->Rq = Rq;
+  Q->inexact = R.inexact;
+  if (share) {
+    Q->Qp = R.Rp;
+    Q->qset = R.sset;
   } else {
     if (dp4s * 4 == d && (reinterpret_cast<uintptr_t>(q) & 15) == 0) {
-      Qp = reinterpret_cast<const float4 *>(q);
+      Q->Qp = reinterpret_cast<const float4 *>(q);
     } else {
       float4 *p;
       KNN_TRY(ar.alloc(&p, (size_t)m * dp4s));
       KNN_TRY(launch_pack_rows(q, m, d, dp4s, p, s));
-      Qp = p;
+      Q->Qp = p;
     }
     int *qf = reinterpret_cast<int *>(ctr + kCtrInexactQ);
-    KNN_TRY(launch_exact_check(reinterpret_cast<const float *>(Qp), m * dp4s * 4, d, qf, s));
-    q_inexact = qf;
-    KNN_TRY(build_clusters(ar, ar, Qp, m, d, dp4s, Rq, o.seed, o.rep_trials, o.lloyd_iters,
-                           use_tc, dev_err, s, &qset));
+    KNN_TRY(launch_exact_check(reinterpret_cast<const float *>(Q->Qp), m * dp4s * 4, d, qf, s));
+    Q->inexact = qf;
+    KNN_TRY(build_clusters(ar, ar, Q->Qp, m, d, dp4s, Rq, o.seed, o.rep_trials, o.lloyd_iters,
+                           use_tc, dev_err, s, &Q->qset));
   }
-  float *qrad, *drr, *theta0;
-  int32_t *slot_cl, *rlist, *rlen;
-  KNN_TRY(ar.alloc(&qrad, (size_t)Rq));
-  KNN_TRY(ar.alloc(&slot_cl, (size_t)m));
-  KNN_TRY(launch_query_clusters(qset.skeys, qset.off, m, Rq, qrad, slot_cl, s));
-  KNN_TRY(ar.alloc(&drr, (size_t)Rq * Rs));
-  KNN_TRY(launch_rep_dist(qset.reps, Rq, sset.reps, Rs, dp4s, drr, s));
-  KNN_TRY(ar.alloc(&theta0, (size_t)Rq));
-  KNN_TRY(ar.alloc(&rlist, (size_t)Rq * Rs));
-  KNN_TRY(ar.alloc(&rlen, (size_t)Rq));
-  KNN_TRY(launch_bounds_filter(drr, Rq, Rs, qrad, qset.off, sset.off, sdist, cmax,
-                               k, d, theta0, rlist, rlen, s));
-  KNN_TRY(evs.record(1, s));
+  KNN_TRY(ar.alloc(&Q->qrad, (size_t)Rq));
+  KNN_TRY(ar.alloc(&Q->slot_cl, (size_t)m));
+  KNN_TRY(launch_query_clusters(Q->qset.skeys, Q->qset.off, m, Rq, Q->qrad, Q->slot_cl, s));
+  KNN_TRY(ar.alloc(&Q->drr, (size_t)Rq * Rs));
+  KNN_TRY(launch_rep_dist(Q->qset.reps, Rq, R.sset.reps, Rs, dp4s, Q->drr, s));
+  KNN_TRY(ar.alloc(&Q->theta0, (size_t)Rq));
+  KNN_TRY(ar.alloc(&Q->rlist, (size_t)Rq * Rs));
+  KNN_TRY(ar.alloc(&Q->rlen, (size_t)Rq));
+  KNN_TRY(launch_bounds_filter(Q->drr, Rq, Rs, Q->qrad, Q->qset.off, R.sset.off, R.sdist, R.cmax,
+                               k, d, Q->theta0, Q->rlist, Q->rlen, s));
+  return KNN_OK;
+}
+
+// The search of the query clusters c0 .. c1-1, whose slots are
+// slot0 .. slot0+nslot-1: the BF16 tile search (precision BF16_REFINE) and
+// the FP32 scan, results into rows of out_idx / out_dist (query order).
+// `ctr` (kCtrCount counters, zeroed) on the searching device.  With a host
+// sink and the whole query set, the scan runs in row chunks whose results
+// are copied back while the next chunk runs.
+int search_clusters(const RefSide &R, const QuerySide &Q, int64_t m, int32_t k, int c0, int c1,
+                    int64_t slot0, int64_t nslot, int32_t *out_idx, float *out_dist,
+                    const knn_options &o, cudaStream_t s, HostSink *sink, Arena &ar,
+                    unsigned long long *ctr) {
+  if (nslot == 0) return KNN_OK;
+  const int d = R.d, dp4s = R.dp4s, Rs = R.Rs;
+  int dev = 0, num_sms = 148;
+  KNN_CUDA_TRY(cudaGetDevice(&dev));
+  KNN_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+  const int nclu = c1 - c0;
 
   // BF16+refine form: tensor-core tiles over the same candidate lists; the
   // FP32 scan below then runs only for the queries the tiles hand back.
@@ -534,38 +439,38 @@ int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t 
   int32_t *fb_slots = nullptr;
   unsigned *fb_count = reinterpret_cast<unsigned *>(ctr + kCtrFallback);
   if (tiles) {
-    grid = (int)std::min<int64_t>(grid, m / 128 + Rq + 1);
+    grid = (int)std::min<int64_t>(grid, nslot / 128 + nclu + 1);
     int32_t *tile_list, *ntiles;
     float2 *buf_lu;
     int32_t *buf_pos;
     const size_t slots = (size_t)grid * 128 * cap;
-    KNN_TRY(ar.alloc(&tile_list, (size_t)4 * (m / 128 + Rq + 1)));
+    KNN_TRY(ar.alloc(&tile_list, (size_t)4 * (nslot / 128 + nclu + 1)));
     KNN_TRY(ar.alloc(&ntiles, 1));
     KNN_TRY(ar.alloc(&buf_lu, slots));
     KNN_TRY(ar.alloc(&buf_pos, slots));
-    KNN_TRY(ar.alloc(&fb_slots, (size_t)m));
-    KNN_TRY(launch_tile_list(qset.off, Rq, tile_list, ntiles, s));
+    KNN_TRY(ar.alloc(&fb_slots, (size_t)nslot));
+    KNN_TRY(launch_tile_list(Q.qset.off + c0, nclu, c0, tile_list, ntiles, s));
     TileArgs t{};
-    t.qrows = Qp;
+    t.qrows = Q.Qp;
     t.dp4 = dp4s;
     t.d = d;
     t.KD = 16;
     while (t.KD < d) t.KD <<= 1;
-    t.qorder = qset.perm;
+    t.qorder = Q.qset.perm;
     t.tiles = tile_list;
     t.ntiles = ntiles;
-    t.srows = srows;
-    t.sidx = sidx;
-    t.rrows = Rp;
-    t.soff = sset.off;
-    t.sdist = sdist;
-    t.cmin = cmin;
-    t.cmax = cmax;
-    t.sreps = sset.reps;
-    t.rlist = rlist;
-    t.rlen = rlen;
+    t.srows = R.srows;
+    t.sidx = R.sidx;
+    t.rrows = R.Rp;
+    t.soff = R.sset.off;
+    t.sdist = R.sdist;
+    t.cmin = R.cmin;
+    t.cmax = R.cmax;
+    t.sreps = R.sset.reps;
+    t.rlist = Q.rlist;
+    t.rlen = Q.rlen;
     t.Rs = Rs;
-    t.theta0 = theta0;
+    t.theta0 = Q.theta0;
     t.k = k;
     t.cap = cap;
     t.P = P;
@@ -577,40 +482,41 @@ int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t 
     t.work = ctr + kCtrTileWork;
     t.fb_slots = fb_slots;
     t.fb_count = fb_count;
-    t.err = dev_err;
+    t.err = reinterpret_cast<int *>(ctr + kCtrErr);
     t.counters = ctr + kCtrTile;
     KNN_TRY(launch_tile_search(t, grid, smem, s));
   }
 
   ScanArgs a{};
-  a.qrows = Qp;
-  a.qorder = qset.perm;
-  a.slot_cl = slot_cl;
-  a.m = m;
+  a.qrows = Q.Qp;
+  a.qorder = Q.qset.perm;
+  a.slot_cl = Q.slot_cl;
+  a.m = nslot;
+  a.slot_base = slot0;
   a.d = d;
   a.dp4 = dp4s;
-  a.dp4_tmpl = tmpl;
+  a.dp4_tmpl = R.tmpl;
   a.k = k;
-  a.idx_in_row = idx_in_row;
+  a.idx_in_row = R.idx_in_row;
   a.squared = (o.flags & KNN_SQUARED_DIST) != 0;
-  a.sreps = sset.reps;
-  a.srows = srows;
-  a.sdist = sdist;
-  a.sidx = sidx;
-  a.soff = sset.off;
-  a.cmin = cmin;
-  a.cmax = cmax;
-  a.theta0 = theta0;
-  a.rlist = rlist;
-  a.rlen = rlen;
+  a.sreps = R.sset.reps;
+  a.srows = R.srows;
+  a.sdist = R.sdist;
+  a.sidx = R.sidx;
+  a.soff = R.sset.off;
+  a.cmin = R.cmin;
+  a.cmax = R.cmax;
+  a.theta0 = Q.theta0;
+  a.rlist = Q.rlist;
+  a.rlen = Q.rlen;
   a.Rs = Rs;
-  a.n_ref = n;
-  a.rrows = Rp;
+  a.n_ref = R.n;
+  a.rrows = R.Rp;
   a.inexact_r = R.inexact;
-  a.inexact_q = q_inexact;
+  a.inexact_q = Q.inexact;
   a.out_idx = out_idx;
   a.out_dist = out_dist;
-  KNN_TRY(ar.alloc(&a.unres_slot, (size_t)m));
+  KNN_TRY(ar.alloc(&a.unres_slot, (size_t)nslot));
   a.unres_count = reinterpret_cast<unsigned *>(ctr + kCtrUnres);
   a.work_counter = ctr + kCtrWork;
   a.counters = ctr + kCtrScan;
@@ -622,7 +528,9 @@ int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t 
   // slots still in query-cluster order) and copy every finished chunk back
   // while the next one runs
   const int64_t out_bytes = m * (int64_t)k * 8;
-  const int nchunks = (sink && !tiles && out_bytes >= (16 << 20) && m >= 8 * 1024) ? 8 : 1;
+  const bool whole = slot0 == 0 && nslot == m;
+  const int nchunks =
+      (sink && whole && !tiles && out_bytes >= (16 << 20) && m >= 8 * 1024) ? 8 : 1;
   ChunkEvents cev;
   if (nchunks > 1) {
     const int chunk_rows = (int)((m + nchunks - 1) / nchunks);
@@ -643,8 +551,8 @@ int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t 
     for (int c = 0; c < nchunks; c++)
       counts[c] = (int32_t)std::max<int64_t>(0, std::min<int64_t>(chunk_rows, m - (int64_t)c * chunk_rows));
     KNN_TRY(upload_i32(counts, ccount, s));
-    KNN_TRY(launch_chunk_slots(qset.perm, m, chunk_rows, nchunks, ckeys, ckeys_out, cvals, cslots,
-                               ctemp, tb, s));
+    KNN_TRY(launch_chunk_slots(Q.qset.perm, m, chunk_rows, nchunks, ckeys, ckeys_out, cvals,
+                               cslots, ctemp, tb, s));
     cev.ev.assign(nchunks, nullptr);
     for (int c = 0; c < nchunks; c++) {
       if (counts[c] == 0) continue;
@@ -668,29 +576,49 @@ int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t 
   } else {
     KNN_TRY(launch_scan(a, num_sms, s));
   }
-  KNN_TRY(evs.record(2, s));
+  return KNN_OK;
+}
 
+// Copies the device counters of one call into `st` (synchronises `s`).
+int read_stats(const unsigned long long *ctr, cudaStream_t s, knn_stats *st) {
+  unsigned long long h[kCtrCount];
+  KNN_CUDA_TRY(cudaMemcpyAsync(h, ctr, sizeof h, cudaMemcpyDeviceToHost, s));
+  KNN_CUDA_TRY(cudaStreamSynchronize(s));
+  if (static_cast<int>(h[kCtrErr] & 0xffffffffu) != 0) {
+    set_error("a bounded device wait gave up (tensor-core pipeline)");
+    return KNN_ETIMEOUT;
+  }
+  const unsigned long long *sc = h + kCtrScan, *tc = h + kCtrTile;
+  st->dist_evals += (int64_t)(sc[0] + tc[0] + tc[1]);
+  st->fp64_rechecks += (int64_t)(sc[5] + tc[2]);
+  st->refine_fallbacks += (int32_t)tc[3];
+  st->band_queries += (int32_t)sc[6];
+  st->clusters_visited += (int64_t)sc[1];
+  st->clusters_pruned += (int64_t)sc[2];
+  st->topk_candidates += (int64_t)sc[3];
+  st->topk_merges += (int64_t)sc[4];
+  return KNN_OK;
+}
+
+// The query side of a join against a built reference side.  `ctr`
+// (kCtrCount counters, zeroed) and the events come from the caller; event 0
+// is recorded.
+int query_impl(const RefSide &R, bool share, const float *q, int64_t m, int32_t k,
+               int32_t *out_idx, float *out_dist, const knn_options &o, knn_stats *st,
+               cudaStream_t s, HostSink *sink, Arena &ar, EventSet &evs,
+               unsigned long long *ctr) {
+  if (st) st->pairs_total = m * R.n;
+  QuerySide Q;
+  KNN_TRY(build_query_side(R, share, q, m, k, o, ar, ctr, s, &Q));
+  KNN_TRY(evs.record(1, s));
+  KNN_TRY(search_clusters(R, Q, m, k, 0, Q.Rq, 0, m, out_idx, out_dist, o, s, sink, ar, ctr));
+  KNN_TRY(evs.record(2, s));
   if (st) {
-    unsigned long long h[kCtrCount];
-    KNN_CUDA_TRY(cudaMemcpyAsync(h, ctr, sizeof h, cudaMemcpyDeviceToHost, s));
-    KNN_CUDA_TRY(cudaStreamSynchronize(s));
+    KNN_TRY(read_stats(ctr, s, st));
     if (sink && sink->done) KNN_CUDA_TRY(cudaStreamSynchronize(sink->copy));
-    if (static_cast<int>(h[kCtrErr] & 0xffffffffu) != 0) {
-      set_error("a bounded device wait gave up (tensor-core pipeline)");
-      return KNN_ETIMEOUT;
-    }
-    const unsigned long long *sc = h + kCtrScan, *tc = h + kCtrTile;
-    st->dist_evals = (int64_t)(sc[0] + tc[0] + tc[1]);
-    st->fp64_rechecks = (int64_t)(sc[5] + tc[2]);
-    st->refine_fallbacks = (int32_t)tc[3];
-    st->band_queries = (int32_t)sc[6];
-    st->clusters_visited = (int64_t)sc[1];
-    st->clusters_pruned = (int64_t)sc[2];
-    st->topk_candidates = (int64_t)sc[3];
-    st->topk_merges = (int64_t)sc[4];
     st->pairs_pruned = st->pairs_total - st->dist_evals;
-    st->qreps_used = Rq;
-    st->sreps_used = Rs;
+    st->qreps_used = Q.Rq;
+    st->sreps_used = R.Rs;
     st->kernels_launched = launch_counter();
     KNN_CUDA_TRY(cudaEventElapsedTime(&st->ms_build, evs.ev[0], evs.ev[1]));
     KNN_CUDA_TRY(cudaEventElapsedTime(&st->ms_search, evs.ev[1], evs.ev[2]));
@@ -731,7 +659,6 @@ int index_build_impl(const float *r, int64_t n, int32_t d, const knn_options &o,
   return rc;
 }
 
-}  // namespace
 }  // namespace knnsweet
 
 using namespace knnsweet;

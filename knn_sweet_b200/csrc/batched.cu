@@ -761,3 +761,74 @@ extern "C" int knn_join_batched_device(const float *q, const int64_t *q_offsets,
   return batched_impl(q, q_offsets, r, r_offsets, ncloud, d, k, out_idx, out_dist, o, alpha, st,
                       s);
 }
+
+// Host-buffer form (the reference's per-run host arrays, src/knnjoin.cu:
+// 1003-1033, for many runs at once): copies the clouds in on a stream of its
+// own, joins them with knn_join_batched_device and copies the result back.
+extern "C" int knn_join_batched(const float *q, const int64_t *q_offsets, const float *r,
+                                const int64_t *r_offsets, int32_t ncloud, int32_t d, int32_t k,
+                                int32_t *out_idx, float *out_dist, const knn_options *opt,
+                                knn_stats *st) {
+  error_buffer().clear();
+  if (st) memset(st, 0, sizeof *st);
+  if (ncloud < 0 || d <= 0 || k <= 0 || !q_offsets || !r_offsets) {
+    set_error("batched join: need ncloud >= 0, d > 0, k > 0 and host offsets");
+    return KNN_EINVAL;
+  }
+  if (ncloud == 0) return KNN_OK;
+  const int64_t m = q_offsets[ncloud], n = r_offsets[ncloud];
+  if (m < 0 || n < 0 || m > INT32_MAX || n > INT32_MAX) {
+    set_error("batched join: offsets must stay in [0, 2^31)");
+    return KNN_EINVAL;
+  }
+  if (m == 0) {
+    // the device entry point validates the rest; no buffers are touched
+    return knn_join_batched_device(nullptr, q_offsets, nullptr, r_offsets, ncloud, d, k, nullptr,
+                                   nullptr, opt, st, nullptr);
+  }
+  if (!q || (!r && n > 0) || !out_idx || !out_dist) {
+    set_error("batched join: null pointer argument");
+    return KNN_EINVAL;
+  }
+  const bool self = q == r && std::equal(q_offsets, q_offsets + ncloud + 1, r_offsets);
+  cudaStream_t s;
+  KNN_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  int rc = KNN_OK;
+  {
+    BatchArena ar(s);
+    float *dq = nullptr, *dr = nullptr, *dd = nullptr;
+    int32_t *di = nullptr;
+    rc = ar.alloc(&dq, (size_t)m * d);
+    if (rc == KNN_OK && !self) rc = ar.alloc(&dr, (size_t)n * d);
+    if (rc == KNN_OK) rc = ar.alloc(&di, (size_t)m * k);
+    if (rc == KNN_OK) rc = ar.alloc(&dd, (size_t)m * k);
+    if (self) dr = dq;
+    cudaError_t e = cudaSuccess;
+    if (rc == KNN_OK) e = cudaMemcpyAsync(dq, q, sizeof(float) * m * d, cudaMemcpyHostToDevice, s);
+    if (rc == KNN_OK && e == cudaSuccess && !self && n > 0)
+      e = cudaMemcpyAsync(dr, r, sizeof(float) * n * d, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+      set_error("host-to-device copy failed: %s", cudaGetErrorString(e));
+      rc = KNN_ECUDA;
+    }
+    if (rc == KNN_OK)
+      rc = knn_join_batched_device(dq, q_offsets, dr, r_offsets, ncloud, d, k, di, dd, opt, st,
+                                   s);
+    if (rc == KNN_OK) {
+      e = cudaMemcpyAsync(out_idx, di, sizeof(int32_t) * m * k, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out_dist, dd, sizeof(float) * m * k, cudaMemcpyDeviceToHost, s);
+      if (e != cudaSuccess) {
+        set_error("device-to-host copy failed: %s", cudaGetErrorString(e));
+        rc = KNN_ECUDA;
+      }
+    }
+  }
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess && rc == KNN_OK) {
+    set_error("batched join failed on the device: %s", cudaGetErrorString(e));
+    rc = KNN_ECUDA;
+  }
+  cudaStreamDestroy(s);
+  return rc;
+}

@@ -565,6 +565,62 @@ __global__ void exact_check_kernel(const float *__restrict__ x, int64_t count, f
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(inexact, 1);
 }
 
+// Estimated search work of every query cluster, to balance a partition of
+// the query clusters across devices (the reference runs its whole search on
+// one GPU, src/knnjoin.cu:1103-1129): the cluster's query count times the
+// summed sizes of the bands it can scan, each taken for the cluster as a
+// whole (members s of a surviving reference cluster Rs with
+// |d(Rq,Rs) - d(s,Rs)| <= rq + theta0), plus one per query.  One warp per
+// query cluster.
+__global__ void cluster_work_kernel(const float *__restrict__ drr, int Rq, int Rs,
+                                    const float *__restrict__ qrad,
+                                    const float *__restrict__ theta0,
+                                    const int32_t *__restrict__ qoff,
+                                    const int32_t *__restrict__ rlist,
+                                    const int32_t *__restrict__ rlen,
+                                    const int32_t *__restrict__ soff,
+                                    const float *__restrict__ sdist, long long *__restrict__ work) {
+  const int lane = threadIdx.x & 31;
+  const int qc = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (qc >= Rq) return;
+  const float w = qrad[qc] + theta0[qc];
+  long long band = 0;
+  for (int j = lane; j < rlen[qc]; j += 32) {
+    const int rs = rlist[(int64_t)qc * Rs + j];
+    const float D = drr[(int64_t)qc * Rs + rs];
+    const int a = soff[rs], n = soff[rs + 1] - a;
+    int lo = 0, hi = n;  // first member >= D - w
+    while (lo < hi) {
+      const int md = (lo + hi) >> 1;
+      if (sdist[a + md] < D - w) lo = md + 1;
+      else hi = md;
+    }
+    int l2 = lo, h2 = n;  // first member > D + w
+    while (l2 < h2) {
+      const int md = (l2 + h2) >> 1;
+      if (sdist[a + md] <= D + w) l2 = md + 1;
+      else h2 = md;
+    }
+    band += l2 - lo;
+  }
+  for (int o = 16; o > 0; o >>= 1) band += __shfl_xor_sync(0xffffffffu, band, o);
+  if (lane == 0) {
+    const long long nq = qoff[qc + 1] - qoff[qc];
+    work[qc] = nq * (band + 1);
+  }
+}
+
+int launch_cluster_work(const float *drr, int Rq, int Rs, const float *qrad, const float *theta0,
+                        const int32_t *qoff, const int32_t *rlist, const int32_t *rlen,
+                        const int32_t *soff, const float *sdist, long long *work,
+                        cudaStream_t s) {
+  if (Rq == 0) return KNN_OK;
+  cluster_work_kernel<<<(Rq + 7) / 8, 256, 0, s>>>(drr, Rq, Rs, qrad, theta0, qoff, rlist, rlen,
+                                                 soff, sdist, work);
+  KNN_LAUNCH_CHECK();
+  return KNN_OK;
+}
+
 int launch_exact_check(const float *x, int64_t count, int d, int *inexact, cudaStream_t s) {
   if (count == 0) return KNN_OK;
   const float bound = floorf(sqrtf(16777216.0f / (float)d) * 0.5f);

@@ -35,7 +35,8 @@ struct ScanArgs {
   const int64_t *qc_ref_base;  // batched form: subtracted from every output
                                // index of query cluster qc (null: 0)
   const int32_t *slot_list;    // optional: scan only these slots ...
-  const unsigned *slot_count;  // ... *slot_count of them (device count)
+  const unsigned *slot_count;  // ... *slot_count of them (device count);
+  int64_t slot_base;           // without a list: slots slot_base .. + m - 1
   int Rs;
   int64_t n_ref;            // reference points (0: unknown); with Rs it gives
                             // the mean cluster size the scan variant is chosen by
@@ -58,6 +59,11 @@ int launch_pack_rows(const float *src, int64_t n, int d, int dp4, float4 *dst,
 // Raises *inexact unless every value of x[0..count) is an integer small enough
 // that FP32 squared distances in dimension d are exact.
 int launch_exact_check(const float *x, int64_t count, int d, int *inexact, cudaStream_t s);
+// Estimated search work per query cluster (for partitioning across devices).
+int launch_cluster_work(const float *drr, int Rq, int Rs, const float *qrad, const float *theta0,
+                        const int32_t *qoff, const int32_t *rlist, const int32_t *rlen,
+                        const int32_t *soff, const float *sdist, long long *work,
+                        cudaStream_t s);
 int launch_rep_select(const float4 *rows, int dp4, const int32_t *cand_dev,
                       int R, int trials, uint32_t *score_dev, float4 *reps,
                       int32_t *rep_rows, cudaStream_t s);
@@ -135,7 +141,9 @@ struct TileArgs {
 bool tile_search_supported(int d, int k, int margin);
 int tile_search_geometry(int d, int k, int margin, int num_sms, int *grid, int *cap, int *P,
                          size_t *smem);
-int launch_tile_list(const int32_t *qoff, int Rq, int32_t *tiles, int32_t *ntiles,
+// Tiles of the query clusters c_base .. c_base + Rq - 1 (qoff points at
+// c_base's offset; the tiles carry absolute cluster ids and slots).
+int launch_tile_list(const int32_t *qoff, int Rq, int c_base, int32_t *tiles, int32_t *ntiles,
                      cudaStream_t s);
 int launch_tile_search(const TileArgs &a, int grid, size_t smem, cudaStream_t s);
 

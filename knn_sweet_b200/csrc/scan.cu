@@ -572,6 +572,8 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
       slot = a.slot_list[slot];
     } else if (slot >= a.m) {
       break;
+    } else {
+      slot += a.slot_base;
     }
     const int64_t q = a.qorder[slot];
     const int qc = a.slot_cl[slot];
@@ -858,7 +860,7 @@ __global__ void __launch_bounds__(256, 4)
   const int64_t nslots = a.slot_list ? (int64_t)*a.slot_count : a.m;
   unsigned evals = 0, visited = 0, pruned = 0, pushed = 0;
   if (t < nslots) {
-    const int64_t slot = a.slot_list ? (int64_t)a.slot_list[t] : t;
+    const int64_t slot = a.slot_list ? (int64_t)a.slot_list[t] : a.slot_base + t;
     const int64_t q = a.qorder[slot];
     const int qc = a.slot_cl[slot];
     const int d = a.d;

@@ -70,8 +70,8 @@ constexpr int kTN = 128;  // member rows per chunk: TMEM columns
 // The centre is the cluster's first slot: the query nearest its
 // representative.  One block of 1024 threads, each owning a run of clusters.
 __global__ void __launch_bounds__(1024)
-    tile_list_kernel(const int32_t *__restrict__ qoff, int Rq, int32_t *__restrict__ tiles,
-                     int32_t *__restrict__ ntiles) {
+    tile_list_kernel(const int32_t *__restrict__ qoff, int Rq, int c_base,
+                     int32_t *__restrict__ tiles, int32_t *__restrict__ ntiles) {
   __shared__ int wsum[32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int per = (Rq + 1023) / 1024;
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(1024)
   for (int c = c0; c < c1; c++) {
     const int size = qoff[c + 1] - qoff[c];
     for (int s = 0; s < size; s += kTM) {
-      tiles[4 * pos + 0] = c;
+      tiles[4 * pos + 0] = c_base + c;
       tiles[4 * pos + 1] = qoff[c] + s;
       tiles[4 * pos + 2] = min(kTM, size - s);
       tiles[4 * pos + 3] = qoff[c];
@@ -831,9 +831,9 @@ int tile_search_geometry(int d, int k, int margin, int num_sms, int *grid, int *
   return KNN_OK;
 }
 
-int launch_tile_list(const int32_t *qoff, int Rq, int32_t *tiles, int32_t *ntiles,
+int launch_tile_list(const int32_t *qoff, int Rq, int c_base, int32_t *tiles, int32_t *ntiles,
                      cudaStream_t s) {
-  tile_list_kernel<<<1, 1024, 0, s>>>(qoff, Rq, tiles, ntiles);
+  tile_list_kernel<<<1, 1024, 0, s>>>(qoff, Rq, c_base, tiles, ntiles);
   KNN_LAUNCH_CHECK();
   return KNN_OK;
 }

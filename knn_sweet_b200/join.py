@@ -159,9 +159,10 @@ def knnjoin_sharded(queries, sources=None, k: int = 200, *, devices=(0,), qreps:
                     sreps: int = 0, seed: int = 2015, rep_trials: int = 10,
                     precision: str = "fp32", margin: int = 32, stats: bool = False, out=None,
                     squared: bool = False, tensor_cores: bool = True, lloyd_iters: int = 0):
-    """knnjoin over several GPUs of this process (knn_join_sharded): the queries
-    are split into len(devices) contiguous ranges, each device builds the
-    reference index and joins its range; the result is knnjoin's.  Host
+    """knnjoin over several GPUs of this process (knn_join_sharded): the index
+    and query clusters are built once on devices[0], the query clusters split
+    into len(devices) ranges balanced by estimated work, each device searches
+    its range from a peer copy of the index; the result is knnjoin's.  Host
     (numpy) arrays in and out; a device id may repeat."""
     lib = _lib.load()
     opt = _options(qreps, sreps, seed, rep_trials, precision, margin, squared, tensor_cores,
@@ -190,6 +191,46 @@ def knnjoin_sharded(queries, sources=None, k: int = 200, *, devices=(0,), qreps:
     if stats:
         return idx, dist, JoinStats(**st.as_dict())
     return idx, dist
+
+
+def knnjoin_partition(queries, sources=None, k: int = 200, *, part: int, nparts: int,
+                      qreps: int = 0, sreps: int = 0, seed: int = 2015, rep_trials: int = 10,
+                      precision: str = "fp32", margin: int = 32, stats: bool = False,
+                      squared: bool = False, tensor_cores: bool = True, lloyd_iters: int = 0):
+    """Part `part` of `nparts` of the join (knn_join_partition_device), for one
+    process per GPU: every process passes the same CUDA tensors and options;
+    each builds the same index, takes its share of the query clusters and
+    returns (idx, dist, rows): full (m, k) tensors in which the rows listed in
+    `rows` (int32, this part's queries) hold their results."""
+    import torch
+    lib = _lib.load()
+    opt = _options(qreps, sreps, seed, rep_trials, precision, margin, squared, tensor_cores,
+                   lloyd_iters)
+    st = _lib.KnnStats()
+    q = queries.detach().contiguous()
+    r = q if sources is None else sources.detach().contiguous()
+    if not q.is_cuda or q.dtype != torch.float32 or q.dim() != 2:
+        raise ValueError("queries must be a 2-D float32 CUDA tensor")
+    if r.dtype != torch.float32 or r.dim() != 2 or r.shape[1] != q.shape[1] or r.device != q.device:
+        raise ValueError("sources must be a 2-D float32 tensor with the queries' d and device")
+    m, d = q.shape
+    idx = torch.empty((m, k), dtype=torch.int32, device=q.device)
+    dist = torch.empty((m, k), dtype=torch.float32, device=q.device)
+    rows = torch.empty((m,), dtype=torch.int32, device=q.device)
+    count = ctypes.c_int64(0)
+    with torch.cuda.device(q.device):
+        stream = torch.cuda.current_stream(q.device).cuda_stream
+        rc = lib.knn_join_partition_device(
+            ctypes.c_void_p(q.data_ptr()), m, ctypes.c_void_p(r.data_ptr()), r.shape[0], d, k,
+            int(part), int(nparts), ctypes.c_void_p(idx.data_ptr()),
+            ctypes.c_void_p(dist.data_ptr()), ctypes.c_void_p(rows.data_ptr()),
+            ctypes.byref(count), ctypes.byref(opt), ctypes.byref(st) if stats else None,
+            ctypes.c_void_p(stream))
+    _lib.check(rc)
+    rows = rows[:count.value]
+    if stats:
+        return idx, dist, rows, JoinStats(**st.as_dict())
+    return idx, dist, rows
 
 
 def pack_indexdist(idx: np.ndarray, dist: np.ndarray) -> np.ndarray:

@@ -51,3 +51,47 @@ def test_two_gloo_ranks_agree_on_timing(tmp_path):
         assert x["ms"] == 20.0                      # the slowest rank's time, everywhere
         assert x["value"] == pytest.approx(2 * 1000 / 0.020)
         assert x["rc"] == 0
+
+
+def _gather_worker(rank, world, port, out_dir):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, str(ROOT))
+    import bench
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world, timeout=datetime.timedelta(seconds=60))
+    m, k = 11, 3
+    # uneven parts, as the work-balanced partition gives: rank 0 takes the
+    # rows divisible by 3, rank 1 the rest
+    rows = torch.tensor([i for i in range(m) if (i % 3 == 0) == (rank == 0)], dtype=torch.int32)
+    ri = (rows[:, None] * 10 + torch.arange(k, dtype=torch.int32)[None, :]).to(torch.int32)
+    rd = ri.to(torch.float32) / 4
+    got = bench.gather_rows(dist, rows, ri, rd, m, k, "cpu")
+    ok = True
+    if rank == 0:
+        want = torch.arange(m, dtype=torch.int32)[:, None] * 10 + torch.arange(k)[None, :]
+        ok = bool(torch.equal(got[0], want.to(torch.int32))
+                  and torch.equal(got[1], want.to(torch.float32) / 4))
+    else:
+        ok = got is None
+    ms = bench.max_over_ranks(dist, 1.0 + rank, "cpu")
+    dist.barrier()
+    dist.destroy_process_group()
+    Path(out_dir, f"g{rank}.json").write_text(json.dumps(
+        {"ok": ok, "value": bench.strong_scaling_value(m, ms)}))
+
+
+@pytest.mark.timeout(120)
+def test_partitioned_join_rows_gathered_to_rank0(tmp_path):
+    """The multi-GPU bench step: each rank's part of one join (uneven row
+    sets) all-gathered and assembled into the whole result on rank 0; the
+    whole-job value is the query count over the slowest rank's time."""
+    import torch.multiprocessing as mp
+    world = 2
+    mp.start_processes(_gather_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+                       join=True, start_method="spawn")
+    for r in range(world):
+        x = json.loads(Path(tmp_path, f"g{r}.json").read_text())
+        assert x["ok"]
+        assert x["value"] == pytest.approx(11 / 0.002)

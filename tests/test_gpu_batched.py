@@ -161,3 +161,24 @@ def test_graph_capture_cross_join(cuda_device):
     torch.cuda.synchronize()
     assert torch.equal(gi, wi) and torch.equal(gd, wd)
 
+
+
+def test_host_entry_point_equals_device_entry_point(cuda_device, oracle):
+    """knn_join_batched (host buffers, copies inside the call) gives the device
+    entry point's result, for a self-join and a cross join."""
+    import torch
+    pts, off = data.ellipsoid_clouds(nclouds=40, lo=1, hi=3000, seed=31)
+    a = knnjoin_batched(pts, off, k=12, autotune=False)
+    b = knnjoin_batched(torch.from_numpy(pts).cuda(), off, k=12, autotune=False)
+    torch.cuda.synchronize()
+    assert np.array_equal(a[0], b[0].cpu().numpy()) and np.array_equal(a[1], b[1].cpu().numpy())
+    pairs = data.blob_cloud_pairs(npairs=6, lo=10, hi=2000, seed=32)
+    qo = np.concatenate([[0], np.cumsum([len(p[0]) for p in pairs])]).astype(np.int64)
+    ro = np.concatenate([[0], np.cumsum([len(p[1]) for p in pairs])]).astype(np.int64)
+    q = np.concatenate([p[0] for p in pairs])
+    r = np.concatenate([p[1] for p in pairs])
+    hi, hd = knnjoin_batched(q, qo, r, ro, k=5)
+    for c in range(len(pairs)):
+        oi, od = oracle.bruteforce_f64(q[qo[c]:qo[c + 1]], r[ro[c]:ro[c + 1]], 5)
+        assert_sets(hi[qo[c]:qo[c + 1]], oi)
+        np.testing.assert_allclose(hd[qo[c]:qo[c + 1]], od, rtol=1e-5, atol=1e-7)
