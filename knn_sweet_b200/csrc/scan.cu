@@ -51,31 +51,38 @@ namespace knnsweet {
 // band.  At the end of the query the band is re-decided in FP64
 // (band_resolve_fp64); a query that lost a band key goes to the band kernel
 // instead.
+//
+// Register budget: the dimension comes from the kernel parameters where it is
+// needed and `lostmin` lives in a shared-memory word of the warp, so neither
+// occupies a register through the scan loop.
 struct TopKBase {
   uint64_t *buf;  // append buffer (shared memory)
-  int nbuf, nlist, k, d;
+  float *lostmin; // smallest FP32 d^2 dropped for lack of room (+inf: none)
+  int nbuf, nlist, k;
   uint64_t thr;   // a candidate enters iff its key < thr
   float theta;    // distance matching thr (bound for the pruning tests)
-  float lostmin;  // smallest FP32 d^2 dropped for lack of room (+inf: none)
   unsigned pushed = 0, merges = 0;  // statistics of the current query (warp-uniform)
 
-  __device__ __forceinline__ void reset_threshold(float th0) {
+  __device__ __forceinline__ void reset_threshold(float th0, int lane) {
     nbuf = 0;
     nlist = 0;
     theta = th0;
-    lostmin = __int_as_float(0x7f800000);
+    if (lane == 0) *lostmin = __int_as_float(0x7f800000);
     // admits every d^2 <= th0^2, whatever the index
     thr = ((uint64_t)__float_as_uint(th0 * th0) << 32) | 0xffffffffull;
   }
   // threshold once the k-th squared distance is T: the FP32 band above it
-  __device__ __forceinline__ void set_band_threshold(float T) {
+  __device__ __forceinline__ void set_band_threshold(float T, int d) {
     const float W = band_hi(T, d);
     thr = ((uint64_t)__float_as_uint(W) << 32) | 0xffffffffull;
     theta = sqrtf(W);
   }
   // a dropped key's distance word (NaN from an empty key is ignored)
-  __device__ __forceinline__ void note_lost(uint32_t d2bits) {
-    lostmin = fminf(lostmin, __uint_as_float(__reduce_min_sync(kFull, d2bits)));
+  __device__ __forceinline__ void note_lost(uint32_t d2bits, int lane) {
+    const float v = __uint_as_float(__reduce_min_sync(kFull, d2bits));
+    __syncwarp();
+    if (lane == 0) *lostmin = fminf(*lostmin, v);
+    __syncwarp();
   }
 };
 
@@ -86,26 +93,30 @@ template <int E>
 struct RegTopK : TopKBase {
   static constexpr int L = 32 * E;
   static constexpr int kCap = L;  // candidate buffer capacity
-  // append buffer (L keys), L doubles for the FP64 band, 2 pivot words
-  static constexpr int kSmemKeys = 2 * L + 2;
+  // append buffer (L keys), L doubles for the FP64 band, 2 pivot words,
+  // lostmin
+  static constexpr int kSmemKeys = 2 * L + 3;
   static constexpr int kBandScratch = L, kPivot = 2 * L;
   uint64_t v[E];
 
   __device__ __forceinline__ int cap() const { return kCap; }
 
-  __device__ __forceinline__ void init(uint64_t *wsm) { buf = wsm; }
-
-  __device__ __forceinline__ void reset(float th0, int) {
-#pragma unroll
-    for (int j = 0; j < E; j++) v[j] = kKeyMax;
-    reset_threshold(th0);
+  __device__ __forceinline__ void init(uint64_t *wsm) {
+    buf = wsm;
+    lostmin = reinterpret_cast<float *>(wsm + 2 * L + 2);
   }
 
-  __device__ __forceinline__ void make_room(int lane) { flush(lane); }
-  // end of the query: pending candidates merged into the list
-  __device__ __forceinline__ void finish(int lane) { flush(lane); }
+  __device__ __forceinline__ void reset(float th0, int lane) {
+#pragma unroll
+    for (int j = 0; j < E; j++) v[j] = kKeyMax;
+    reset_threshold(th0, lane);
+  }
 
-  __device__ __forceinline__ void flush(int lane) {
+  __device__ __forceinline__ void make_room(int lane, int d) { flush(lane, d); }
+  // end of the query: pending candidates merged into the list
+  __device__ __forceinline__ void finish(int lane, int d) { flush(lane, d); }
+
+  __device__ __forceinline__ void flush(int lane, int d) {
     if (nbuf == 0) return;
     __syncwarp();
     uint64_t b[E];
@@ -125,7 +136,7 @@ struct RegTopK : TopKBase {
       lost = min(lost, (uint32_t)(umax64(v[j], o) >> 32));
       v[j] = umin64(v[j], o);
     }
-    note_lost(lost);
+    note_lost(lost, lane);
     reg_bitonic_merge<E>(v, lane);
     nlist = min(k, nlist + nbuf);
     merges++;
@@ -143,12 +154,12 @@ struct RegTopK : TopKBase {
 #pragma unroll
       for (int j = 0; j < E; j++)
         if (E * lane + j >= k && key_d2(v[j]) > hi) v[j] = kKeyMax;
-      set_band_threshold(T);
+      set_band_threshold(T, d);
     }
   }
 
   // The candidates, sorted, into buf[0..n); returns n.
-  __device__ __forceinline__ int sorted(int lane) {
+  __device__ __forceinline__ int sorted(int lane, int) {
     __syncwarp();
     int n = 0;
 #pragma unroll
@@ -199,7 +210,7 @@ template <int LL>
 struct SelectTopK : TopKBase {
   static constexpr int L = LL;          // final sort length (pow2 >= k)
   static constexpr int kCap = 2 * LL;   // candidate capacity
-  static constexpr int kSmemKeys = 2 * LL + 128;  // keys + 256-word histogram
+  static constexpr int kSmemKeys = 2 * LL + 129;  // keys, 256-word histogram, lostmin
   // after the final sort: LL doubles for the FP64 band behind the sorted
   // keys, the pivot in the histogram's words
   static constexpr int kBandScratch = LL, kPivot = 2 * LL;
@@ -216,13 +227,14 @@ struct SelectTopK : TopKBase {
   __device__ __forceinline__ void init(uint64_t *wsm) {
     buf = wsm;
     hist = reinterpret_cast<uint32_t *>(wsm + 2 * LL);
+    lostmin = reinterpret_cast<float *>(wsm + 2 * LL + 128);
   }
 
-  __device__ __forceinline__ void reset(float th0, int) { reset_threshold(th0); }
+  __device__ __forceinline__ void reset(float th0, int lane) { reset_threshold(th0, lane); }
 
   // Reduce the set to its k smallest keys (no-op with k or fewer) when ties
   // leave no room otherwise; the keys it drops go into lostmin.
-  __device__ __forceinline__ void flush(int lane) {
+  __device__ __forceinline__ void flush(int lane, int d) {
     if (nbuf <= k) return;
     __syncwarp();
     const uint64_t kth = warp_select_kth(buf, nbuf, k, hist, lane);
@@ -240,11 +252,11 @@ struct SelectTopK : TopKBase {
       w += __popc(bm);
     }
     __syncwarp();
-    note_lost(lost);
+    note_lost(lost, lane);
     nbuf = w;  // == k
     nlist = k;
     merges++;
-    set_band_threshold(key_d2(kth));
+    set_band_threshold(key_d2(kth), d);
   }
 
   // Room for more candidates while the query runs: keep every key whose
@@ -253,7 +265,7 @@ struct SelectTopK : TopKBase {
   // selection on the keys' distance words (on data with many equal distances
   // a 64-bit selection spends most of its passes on the index bits of the
   // ties).  Falls back to the exact k-key flush when ties fill the buffer.
-  __device__ __forceinline__ void make_room(int lane) {
+  __device__ __forceinline__ void make_room(int lane, int d) {
     if (nbuf <= k) return;
     __syncwarp();
     const uint32_t T = warp_select_kth_u32(reinterpret_cast<const uint32_t *>(buf) + 1, 2,
@@ -272,23 +284,23 @@ struct SelectTopK : TopKBase {
     __syncwarp();
     nbuf = w;
     if (w > kCap - 32) {
-      flush(lane);
+      flush(lane, d);
       return;
     }
     merges++;
     nlist = k;
-    set_band_threshold(__uint_as_float(T));
+    set_band_threshold(__uint_as_float(T), d);
   }
 
   // End of the query: nothing to do before sorted().
-  __device__ __forceinline__ void finish(int) {}
+  __device__ __forceinline__ void finish(int, int) {}
 
   // The candidates, sorted, into buf[0..n); returns n.  Up to L keys are
   // sorted as they are; beyond that a band-inclusive compaction first, and
   // the exact k-key flush only if ties still leave more than L.
-  __device__ __forceinline__ int sorted(int lane) {
-    if (nbuf > LL) make_room(lane);
-    if (nbuf > LL) flush(lane);
+  __device__ __forceinline__ int sorted(int lane, int d) {
+    if (nbuf > LL) make_room(lane, d);
+    if (nbuf > LL) flush(lane, d);
     __syncwarp();
     if constexpr (LL <= 128) {
       // sorted in registers (E keys per lane; shuffles for the cross-lane
@@ -318,13 +330,13 @@ struct SelectTopK : TopKBase {
 
 // Offer one key per lane (kKeyMax = nothing); warp-collective.
 template <class TK>
-__device__ __forceinline__ void topk_push(TK &tk, uint64_t key, int lane) {
+__device__ __forceinline__ void topk_push(TK &tk, uint64_t key, int lane, int d) {
   bool pass = key < tk.thr;
   unsigned b = __ballot_sync(kFull, pass);
   if (b == 0) return;
   int cnt = __popc(b);
   if (tk.nbuf + cnt > tk.cap()) {
-    tk.make_room(lane);
+    tk.make_room(lane, d);
     pass = key < tk.thr;
     b = __ballot_sync(kFull, pass);
     cnt = __popc(b);
@@ -350,9 +362,10 @@ __device__ __forceinline__ bool fp32_exact(const ScanArgs &a) {
 // reference decides this boundary by a strict-less insertion of FP32
 // distances, src/knnjoin.cu:815-820.)  qf: the query row; rrows: the
 // reference rows in original order (keys carry original indices); dbl:
-// scratch for nhi - nlo doubles; piv: 2 words.  Out of line: it runs for few
-// queries, and inlined it would cost the scan registers.
-__device__ __noinline__ void band_resolve_fp64(uint64_t *s, int nlo, int nhi, int k, int d,
+// scratch for nhi - nlo doubles; piv: 2 words.  Inlined: as an out-of-line
+// call (for the few queries that need it) it cost the k = 200 self-join scan
+// 8 % (5.15 against 4.82 ms), the call's register saves on every query.
+__device__ __forceinline__ void band_resolve_fp64(uint64_t *s, int nlo, int nhi, int k, int d,
                                                int dp4, const float *__restrict__ qf,
                                                const float4 *__restrict__ rrows, double *dbl,
                                                uint64_t *piv, int lane) {
@@ -397,8 +410,9 @@ __device__ __noinline__ void band_resolve_fp64(uint64_t *s, int nlo, int nhi, in
 // results.  Returns the FP64 distances evaluated.
 template <class TK>
 __device__ __forceinline__ unsigned emit_query(TK &tk, const ScanArgs &a, int32_t slot, int64_t q,
-                                               int qc, bool exact32, int lane) {
-  const int n = tk.sorted(lane);
+                                               int qc, int lane) {
+  const int n = tk.sorted(lane, a.d);
+  const bool exact32 = fp32_exact(a);
   uint64_t *s = tk.buf;
   const int k = a.k;
   bool defer = false;
@@ -415,7 +429,7 @@ __device__ __forceinline__ unsigned emit_query(TK &tk, const ScanArgs &a, int32_
       nlo += __popc(__ballot_sync(kFull, v < lo));
       nhi += __popc(__ballot_sync(kFull, v <= hi));
     }
-    if (tk.lostmin <= hi) {
+    if (*tk.lostmin <= hi) {
       defer = true;
     } else if (nhi > k) {
       band_resolve_fp64(s, nlo, nhi, k, a.d, a.dp4,
@@ -551,8 +565,6 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
   TK tk;
   tk.init(keys_base + (size_t)w * TK::kSmemKeys);
   tk.k = a.k;
-  tk.d = a.d;
-  const bool exact32 = fp32_exact(a);
   const float tol = bound_tol(a.d);
   unsigned evals = 0, visited = 0, pruned = 0, checked = 0;
   // small rows: load the member row together with its band distance
@@ -620,7 +632,7 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
           key = make_key(v, idx);
         }
       }
-      topk_push(tk, key, lane);
+      topk_push(tk, key, lane, a.d);
       return dsv;
     };
 
@@ -752,8 +764,8 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
 #endif
       }
     }
-    tk.finish(lane);
-    checked += emit_query(tk, a, (int32_t)slot, q, qc, exact32, lane);
+    tk.finish(lane, a.d);
+    checked += emit_query(tk, a, (int32_t)slot, q, qc, lane);
     if (a.counters) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
