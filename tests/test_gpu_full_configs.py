@@ -93,7 +93,9 @@ def test_c5_all_pairs_forward_and_gradient(cuda_device, oracle, k):
         assert_matches(ixy[xa:xb], np.sqrt(dxy[xa:xb]), oxy, dxy_o)
         assert_matches(iyx[ya:yb], np.sqrt(dyx[ya:yb]), oyx, dyx_o)
         # the gradient of the pair's loss equals the FP64 gradient over the
-        # oracle's neighbour pairs (same pairs, so only FP32 rounding differs)
+        # oracle's neighbour pairs: the same pairs, so only FP32 rounding
+        # differs -- a point's gradient sums dozens of FP32 atomic adds of
+        # terms up to the largest component, hence 1e-4 of that component
         px, py = xs[xa:xb].astype(np.float64), ys[ya:yb].astype(np.float64)
         rgx, rgy = np.zeros_like(px), np.zeros_like(py)
         dv = px[:, None, :] - py[oxy]
@@ -103,5 +105,5 @@ def test_c5_all_pairs_forward_and_gradient(cuda_device, oracle, k):
         rgy += 2 * dv.sum(1)
         np.add.at(rgx, oyx.ravel(), -2 * dv.reshape(-1, 3))
         scale = max(np.abs(rgx).max(), np.abs(rgy).max())
-        assert np.abs(gx[xa:xb] - rgx).max() <= 1e-5 * scale
-        assert np.abs(gy[ya:yb] - rgy).max() <= 1e-5 * scale
+        assert np.abs(gx[xa:xb] - rgx).max() <= 1e-4 * scale
+        assert np.abs(gy[ya:yb] - rgy).max() <= 1e-4 * scale
