@@ -580,10 +580,13 @@ def form_precision(torch, dev, flush, steps):
     from knn_sweet_b200 import data
     r, q = data.config3()
     k = 100
+    # the representatives are refined (4 centroid steps with the cluster
+    # split), so one random draw seeds them as well as the best of ten
     forms, same = _pair_forms(torch, dev, flush, r, q, k,
-                              dict(qreps=8192, sreps=8192, lloyd_iters=4), steps, 500, 33)
+                              dict(qreps=8192, sreps=8192, lloyd_iters=4, rep_trials=1), steps,
+                              500, 33)
     return {"workload": f"N={r.shape[0]} M={q.shape[0]} d=128 k={k} reps 8192/8192 lloyd 4, "
-                        "synthetic 4,096-Gaussian mixture",
+                        "1 draw trial, synthetic 4,096-Gaussian mixture",
             "fp32": forms["fp32"], "bf16_refine": forms["bf16_refine"],
             "same_neighbor_sets": same,
             "bf16_over_fp32": forms["bf16_refine"]["queries_per_s"] / forms["fp32"]["queries_per_s"]}
@@ -597,9 +600,10 @@ def form_c2(torch, dev, flush, steps):
     r, q = data.config2()
     k = 32
     forms, same = _pair_forms(torch, dev, flush, r, q, k,
-                              dict(qreps=1000, sreps=1000, lloyd_iters=3), steps, 1000, 22)
+                              dict(qreps=1000, sreps=1000, lloyd_iters=3, rep_trials=1), steps,
+                              1000, 22)
     return {"workload": f"N={r.shape[0]} M={q.shape[0]} d=32 k={k} reps 1000/1000 lloyd 3, "
-                        "synthetic 1,000-Gaussian mixture",
+                        "1 draw trial, synthetic 1,000-Gaussian mixture",
             "fp32": forms["fp32"], "bf16_refine": forms["bf16_refine"],
             "same_neighbor_sets": same,
             "bf16_over_fp32": forms["bf16_refine"]["queries_per_s"] / forms["fp32"]["queries_per_s"]}

@@ -507,6 +507,8 @@ int search_clusters(const RefSide &R, const QuerySide &Q, int64_t m, int32_t k, 
   a.cmin = R.cmin;
   a.cmax = R.cmax;
   a.theta0 = Q.theta0;
+  a.qrad = Q.qrad;
+  a.qkeys = Q.qset.skeys;
   a.rlist = Q.rlist;
   a.rlen = Q.rlen;
   a.Rs = Rs;

@@ -550,6 +550,8 @@ int batched_impl(const float *q, const int64_t *qoff_h, const float *r, const in
       a.cmin = cmin;
       a.cmax = cmax;
       a.theta0 = theta0;
+      a.qrad = qrad;
+      a.qkeys = Q.skeys;
       a.rlist = rlist;
       a.rlen = rlen;
       a.rl_base = rl_base;

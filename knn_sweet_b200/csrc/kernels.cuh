@@ -28,6 +28,9 @@ struct ScanArgs {
   const int32_t *soff;      // Rs + 1 cluster offsets
   const float *cmin, *cmax; // Rs: smallest / largest member distance
   const float *theta0;      // Rq: initial k-th bound per query cluster
+  const float *qrad;        // Rq: query cluster radius (the one theta0 used) ...
+  const uint64_t *qkeys;    // ... and slot -> (cluster, d(q, Rq)) sort key: a
+                            // query's own bound theta0 - (rq - d(q,Rq)); null: theta0
   const int32_t *rlist;     // Rq x Rs surviving clusters, nearest first
   const int32_t *rlen;      // Rq
   const int64_t *rl_base;   // batched form: start of each query cluster's list

@@ -344,6 +344,8 @@ int noalloc_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d
   a.cmin = p.cmin;
   a.cmax = p.cmax;
   a.theta0 = p.theta0;
+  a.qrad = p.qrad;
+  a.qkeys = Qb.skeys;
   a.rlist = p.rlist;
   a.rlen = p.rlen;
   a.Rs = p.Rs;

@@ -352,6 +352,25 @@ __device__ __forceinline__ bool fp32_exact(const ScanArgs &a) {
   return a.inexact_r && a.inexact_q && (*a.inexact_r | *a.inexact_q) == 0;
 }
 
+// A query's starting k-th distance bound.  theta0 of its cluster is the k-th
+// smallest of rq + d(Rq,Rs) + d(s,Rs) over the reference points s, rq the
+// cluster's radius; the same k points lie within dq + d(Rq,Rs) + d(s,Rs) of a
+// query at distance dq <= rq from the representative, so theta0 - (rq - dq),
+// widened by the rounding slack, bounds that query's k-th distance too and
+// starts its scan tighter.
+#ifndef KNN_QUERY_THETA0
+#define KNN_QUERY_THETA0 1
+#endif
+__device__ __forceinline__ float query_theta0(const ScanArgs &a, int64_t slot, int qc, float tol) {
+  float th = a.theta0[qc];
+  if (KNN_QUERY_THETA0 && a.qrad && a.qkeys) {
+    const float rq = a.qrad[qc], dq = __uint_as_float((uint32_t)a.qkeys[slot]);
+    const float cut = (rq - dq) - tol * (rq + dq + th);
+    if (cut > 0.0f) th -= cut;
+  }
+  return th;
+}
+
 // FP64 re-decision of one query's k-th boundary, by one warp.  s[0..n) holds
 // the query's candidate keys sorted ascending, n > k; s[0..nlo) lie below the
 // FP32 band of the k-th (band_lo(Dk) .. band_hi(Dk)), s[nlo..nhi) inside it,
@@ -591,7 +610,7 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
     const int qc = a.slot_cl[slot];
     QueryRow<DP4, IDXROW> qr;
     qr.load(a.qrows, q, dp4, qslot);
-    tk.reset(a.theta0[qc], lane);
+    tk.reset(query_theta0(a, slot, qc, tol), lane);
 
     // one band step: lane's member p of the cluster at `start`, kept when
     // its distance to the representative lies in [lo_v, hi_v]
@@ -881,7 +900,7 @@ __global__ void __launch_bounds__(256, 4)
     qr.load(a.qrows, q, DP4, nullptr);
     ThreadTopK<K> tk;
     tk.reset();
-    float theta = a.theta0[qc];
+    float theta = query_theta0(a, slot, qc, tol);
     float lost = __int_as_float(0x7f800000);
     // admits every d^2 <= theta0^2, whatever the index
     const uint64_t thr0 = ((uint64_t)__float_as_uint(theta * theta) << 32) | 0xffffffffull;

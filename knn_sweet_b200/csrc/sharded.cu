@@ -135,6 +135,8 @@ int replicate_sides(Arena &ar, int g, int g0, const RefSide &R, const QuerySide 
   KNN_TRY(replicate(ar, g, g0, Q.qset.off, (size_t)Rq + 1, s, &Q2->qset.off));
   KNN_TRY(replicate(ar, g, g0, Q.slot_cl, (size_t)m, s, &Q2->slot_cl));
   KNN_TRY(replicate(ar, g, g0, Q.theta0, (size_t)Rq, s, &Q2->theta0));
+  KNN_TRY(replicate(ar, g, g0, Q.qrad, (size_t)Rq, s, &Q2->qrad));
+  KNN_TRY(replicate(ar, g, g0, Q.qset.skeys, (size_t)m, s, &Q2->qset.skeys));
   KNN_TRY(replicate(ar, g, g0, Q.rlist, (size_t)Rq * Rs, s, &Q2->rlist));
   KNN_TRY(replicate(ar, g, g0, Q.rlen, (size_t)Rq, s, &Q2->rlen));
   return KNN_OK;

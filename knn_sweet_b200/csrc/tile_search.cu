@@ -62,8 +62,14 @@ __device__ unsigned long long tile_prof[16];
   } while (0)
 #endif
 
-constexpr int kTM = 128;  // queries per tile: TMEM lanes, threads per CTA
+constexpr int kTM = 128;  // queries per tile: TMEM lanes, the row threads of a CTA
 constexpr int kTN = 128;  // member rows per chunk: TMEM columns
+// Threads per CTA (template NT): the first kTM own the tile's rows (TMEM
+// lanes) through the epilogue.  With NT = 2 kTM all of them stage tiles and
+// share out the re-ranking, so that the latency-bound CTA keeps twice the
+// warps in flight at the same shared memory; that pays where the re-ranking
+// state of four more warps fits the tile region (wide rows, d = 128: C3
+// search 16.0 -> 13.2 ms).  Otherwise NT = kTM keeps four CTAs per SM.
 
 // Tile list: every query cluster's slots in tiles of up to kTM, as
 // {query cluster, first slot, count, slot of the cluster's centre point}.
@@ -116,19 +122,19 @@ __global__ void __launch_bounds__(1024)
 //   o_n = sum v^2, o_e = sum (v - bf16(v))^2, o_t = sum bf16(v)^2
 // of the centred FP32 values v.  rowptr(r) gives the row (nullptr: zeros).
 // G = KD/8 consecutive threads share a row (one 16-byte group each).
-template <class RowPtr>
+template <int NT, class RowPtr>
 __device__ __forceinline__ void stage_tile(unsigned char *tile, const float *sc, int KD, int d,
                                            int dp4, RowPtr rowptr, float *o_n, float *o_e,
                                            float *o_t) {
   const int G = KD >> 3;
   // four 16-byte groups per thread per round, their loads issued together
   // (whether a round's group exists depends only on the round: uniform)
-  for (int t0 = threadIdx.x; t0 < kTM * G; t0 += 4 * kTM) {
+  for (int t0 = threadIdx.x; t0 < kTM * G; t0 += 4 * NT) {
     float4 c0[4], c1[4];
     bool has[4];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
-      const int t = t0 + u * kTM;
+      const int t = t0 + u * NT;
       const int r = t / G, k0 = (t - r * G) << 3;
       const float4 *row = t < kTM * G ? rowptr(r) : nullptr;
       has[u] = row != nullptr;
@@ -141,7 +147,7 @@ __device__ __forceinline__ void stage_tile(unsigned char *tile, const float *sc,
     }
 #pragma unroll
     for (int u = 0; u < 4; u++) {
-      const int t = t0 + u * kTM;
+      const int t = t0 + u * NT;
       if (t >= kTM * G) break;
       const int r = t / G, g = t - r * G, k0 = g << 3;
       const float v[8] = {c0[u].x, c0[u].y, c0[u].z, c0[u].w,
@@ -260,8 +266,15 @@ __device__ __forceinline__ void sort_keys_in_registers(uint64_t *s, int n, int l
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(kTM)
+// Bytes of the query and member tiles at the start of shared memory.
+__host__ __device__ constexpr size_t tiles_bytes(int KD) {
+  return tc::tile_bytes(kTM, KD) + tc::tile_bytes(kTN, KD);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT, NT == kTM ? 4 : 2)
     tile_search_kernel(const TileArgs a) {
+  constexpr int kThreads = NT, kWarps = NT / 32;
   extern __shared__ __align__(1024) unsigned char smem[];
   const int KD = a.KD, d = a.d, dp4 = a.dp4, k = a.k, cap = a.cap, P = a.P;
   (void)P;
@@ -281,20 +294,37 @@ __global__ void __launch_bounds__(kTM)
   float *s_ck = s_cmax + kTN;                                    // k-th member distance
   uint32_t *s_blo = reinterpret_cast<uint32_t *>(s_ck + kTN);    // run bounds (float bits)
   uint32_t *s_bhi = s_blo + kTN;
-  int32_t *s_wsum = reinterpret_cast<int32_t *>(s_bhi + kTN);    // 4 warp sums
-  uint32_t *s_wmax = reinterpret_cast<uint32_t *>(s_wsum + 4);   // [1]: run total
+  int32_t *s_wsum = reinterpret_cast<int32_t *>(s_bhi + kTN);    // kWarps warp sums
+  uint32_t *s_wmax = reinterpret_cast<uint32_t *>(s_wsum + kWarps);  // [1]: run total
   uint32_t *hist = s_wmax + 4;                                   // 4 x 256
   uint64_t *mbar = reinterpret_cast<uint64_t *>(hist + 4 * 256);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mbar + 1);
   int32_t *s_tile = reinterpret_cast<int32_t *>(tmem_slot + 1);  // 4 ints
-  // per warp: one query's buffer (cap bound pairs, cap positions)
+  // warps 0-3: one query's buffer each (cap bound pairs, cap positions), a
+  // query row and a histogram, for the compactions between member chunks
+  // and the final re-ranking; warps 4-7 join the re-ranking only, once the
+  // tiles are no longer needed, with the same state inside the tile region
   const size_t wofs = ((size_t)(reinterpret_cast<unsigned char *>(s_tile + 4) - smem) + 15) &
                       ~(size_t)15;
-  float4 *wq = reinterpret_cast<float4 *>(smem + wofs) + (size_t)warp * dp4;
-  unsigned char *wbase = smem + wofs + 4 * (size_t)dp4 * 16 + (size_t)warp * cap * 12;
+  const size_t wstate = (size_t)cap * 12 + (size_t)dp4 * 16 + 256 * 4;  // bytes per warp
+  const bool rerank_all = kWarps > 4 && 4 * wstate <= tiles_bytes(KD);
+  float4 *wq;
+  unsigned char *wbase;
+  uint32_t *whist;
+  if (warp < 4) {
+    wq = reinterpret_cast<float4 *>(smem + wofs) + (size_t)warp * dp4;
+    wbase = smem + wofs + 4 * (size_t)dp4 * 16 + (size_t)warp * cap * 12;
+    whist = hist + warp * 256;
+  } else {
+    unsigned char *w0 = smem + (size_t)(warp - 4) * wstate;
+    wbase = w0;
+    wq = reinterpret_cast<float4 *>(w0 + (size_t)cap * 12);
+    whist = reinterpret_cast<uint32_t *>(w0 + (size_t)cap * 12 + (size_t)dp4 * 16);
+  }
   float2 *w_lu = reinterpret_cast<float2 *>(wbase);
   int32_t *w_pos = reinterpret_cast<int32_t *>(wbase + (size_t)cap * 8);
-  uint32_t *whist = hist + warp * 256;
+  // warps sharing out the final re-ranking
+  const int nrw = rerank_all ? kWarps : 4;
 
   if (warp == 0) tc::tmem_alloc(tmem_slot, kTN);
   if (tid == 0) tc::mbar_init(mbar, 1);
@@ -314,8 +344,9 @@ __global__ void __launch_bounds__(kTM)
   // representative and member distances)
   const float tol = bound_tol(d);
   const size_t row0 = (size_t)blockIdx.x * kTM;
-  float2 *my_lu = a.buf_lu + (row0 + tid) * cap;
-  int32_t *my_pos = a.buf_pos + (row0 + tid) * cap;
+  // this row's global bound buffer (row threads only)
+  float2 *my_lu = a.buf_lu + (row0 + (tid & (kTM - 1))) * cap;
+  int32_t *my_pos = a.buf_pos + (row0 + (tid & (kTM - 1))) * cap;
   uint32_t phase = 0;
   bool ok = true;
   unsigned long long pairs = 0, refined = 0, rechecks = 0, fallbacks = 0;
@@ -340,19 +371,20 @@ __global__ void __launch_bounds__(kTM)
     const int s0 = s_tile[1], cnt = s_tile[2];
     const float *cen = reinterpret_cast<const float *>(a.qrows +
                                                        (size_t)a.qorder[s_tile[3]] * dp4);
-    for (int kk = tid; kk < KD; kk += kTM) sc[kk] = kk < d ? cen[kk] : 0.0f;
+    for (int kk = tid; kk < KD; kk += kThreads) sc[kk] = kk < d ? cen[kk] : 0.0f;
     __syncthreads();
-    stage_tile(
+    stage_tile<NT>(
         sa, sc, KD, d, dp4,
         [&](int r) -> const float4 * {
           return r < cnt ? a.qrows + (size_t)a.qorder[s0 + r] * dp4 : nullptr;
         },
         s_n, s_e, s_t);
     __syncthreads();
+    const bool row_thread = tid < kTM;  // owns tile row (TMEM lane) tid
     const bool valid = tid < cnt;
-    const float na = s_n[tid];
+    const float na = row_thread ? s_n[tid] : 0.0f;
     const float qa = 2.02f * sqrtf(na);
-    const float qb = 2.02f * (sqrtf(s_e[tid]) + gtc * sqrtf(s_t[tid]));
+    const float qb = row_thread ? 2.02f * (sqrtf(s_e[tid]) + gtc * sqrtf(s_t[tid])) : 0.0f;
     const float th = a.theta0[qc];
     float tau = th * th * 1.0009765625f;
     int n = 0;
@@ -382,9 +414,9 @@ __global__ void __launch_bounds__(kTM)
     float *s_uk = s_t;
     auto compact_rows = [&](int above) {
       const bool mine = valid && !ovf && n > above && n >= k;
-      s_req[tid] = mine ? n : 0;
+      if (row_thread) s_req[tid] = mine ? n : 0;
       if (!__syncthreads_or(mine)) return;
-      for (int rr = warp; rr < cnt; rr += 4) {
+      for (int rr = warp; warp < 4 && rr < cnt; rr += 4) {
         const int nn = s_req[rr];
         if (nn == 0) continue;
         const size_t ro = (row0 + rr) * cap;
@@ -412,7 +444,7 @@ __global__ void __launch_bounds__(kTM)
     // bounds before the rest of the list is decided
     for (int jb = 0, nb = 0; jb < nl && ok; jb += nb) {
       nb = jb == 0 ? min(4, nl) : min(kTN, nl - jb);
-      stage_tile(
+      stage_tile<NT>(
           sb, sc, KD, d, dp4,
           [&](int r) -> const float4 * {
             return r < nb ? a.sreps + (size_t)rl[jb + r] * dp4 : nullptr;
@@ -439,8 +471,9 @@ __global__ void __launch_bounds__(kTM)
         }
         tc::mma_commit(mbar);
       }
-      s_col[tid] = tid < nb ? make_float4(s_n[tid], sqrtf(s_e[tid]), sqrtf(s_t[tid]), 0.0f)
-                            : make_float4(__int_as_float(0x7f800000), 0.0f, 0.0f, 0.0f);
+      if (row_thread)
+        s_col[tid] = tid < nb ? make_float4(s_n[tid], sqrtf(s_e[tid]), sqrtf(s_t[tid]), 0.0f)
+                              : make_float4(__int_as_float(0x7f800000), 0.0f, 0.0f, 0.0f);
       ok = tc::mbar_wait(mbar, phase);
       phase ^= 1u;
       ok = __syncthreads_and(ok) != 0;
@@ -448,7 +481,7 @@ __global__ void __launch_bounds__(kTM)
       tc::fence_after_sync();
       const bool act = valid && !ovf;
       // pass 1: tighter theta_q from clusters with >= k members
-      for (int cc = 0; cc < nb; cc += 32) {
+      for (int cc = 0; warp < 4 && cc < nb; cc += 32) {  // TMEM lanes: warps 0-3
         float acc[32];
         tc::tmem_ld_32x32(lane_base + (uint32_t)cc, acc);
         if (act) {
@@ -466,7 +499,7 @@ __global__ void __launch_bounds__(kTM)
       }
       if (act) tau = fminf(tau, th_q * th_q * (1.0f + 4.0f * tol));
       // pass 2: the clusters each query needs and the union of their runs
-      for (int cc = 0; cc < nb; cc += 32) {
+      for (int cc = 0; warp < 4 && cc < nb; cc += 32) {  // TMEM lanes: warps 0-3
         float acc[32];
         tc::tmem_ld_32x32(lane_base + (uint32_t)cc, acc);
         if (act) {
@@ -522,8 +555,10 @@ __global__ void __launch_bounds__(kTM)
         __syncthreads();
         int before = 0;
         for (int w = 0; w < warp; w++) before += s_wsum[w];
-        s_rlo[tid] = lo;
-        s_roff[tid] = before + incl - len;
+        if (row_thread) {
+          s_rlo[tid] = lo;
+          s_roff[tid] = before + incl - len;
+        }
         if (tid == kTM - 1) s_wmax[1] = (uint32_t)(before + incl);
       }
       __syncthreads();
@@ -542,7 +577,7 @@ __global__ void __launch_bounds__(kTM)
       for (int o = 0; o < total; o += kTN) {
         const int nr = min(kTN, total - o);
         const bool last_of_first = jb == 0 && o + kTN >= total;
-        stage_tile(
+        stage_tile<NT>(
             sb, sc, KD, d, dp4,
             [&](int r) -> const float4 * {
               if (r >= nr) return nullptr;
@@ -572,16 +607,17 @@ __global__ void __launch_bounds__(kTM)
           tc::mma_commit(mbar);
         }
         // column scalars: |b|^2 (+inf on padding), |b - b~|, |b~|, position
-        s_col[tid] = tid < nr ? make_float4(s_n[tid], sqrtf(s_e[tid]), sqrtf(s_t[tid]),
-                                            __int_as_float(s_pos[tid]))
-                              : make_float4(__int_as_float(0x7f800000), 0.0f, 0.0f, 0.0f);
+        if (row_thread)
+          s_col[tid] = tid < nr ? make_float4(s_n[tid], sqrtf(s_e[tid]), sqrtf(s_t[tid]),
+                                              __int_as_float(s_pos[tid]))
+                                : make_float4(__int_as_float(0x7f800000), 0.0f, 0.0f, 0.0f);
         ok = tc::mbar_wait(mbar, phase);
         phase ^= 1u;
         ok = __syncthreads_and(ok) != 0;
         if (!ok) break;
         tc::fence_after_sync();
         TILE_PROF(2);
-        for (int cc = 0; cc < nr; cc += 32) {
+        for (int cc = 0; warp < 4 && cc < nr; cc += 32) {  // TMEM lanes: warps 0-3
           float acc[32];
           tc::tmem_ld_32x32(lane_base + (uint32_t)cc, acc);
           if (valid && !ovf) {
@@ -623,13 +659,15 @@ __global__ void __launch_bounds__(kTM)
       atomicAdd(&tile_prof[15], 1ull);
     }
 #endif
-    // finish the tile's queries, shared out over the four warps: exact
-    // re-ranking and the FP64 boundary, on a shared-memory copy of each
-    // query's buffer
-    s_req[tid] = n;
-    s_kept[tid] = ovf ? 1 : 0;
+    // finish the tile's queries, shared out over the warps (all of them when
+    // their state fits the free tile region): exact re-ranking and the FP64
+    // boundary, on a shared-memory copy of each query's buffer
+    if (row_thread) {
+      s_req[tid] = n;
+      s_kept[tid] = ovf ? 1 : 0;
+    }
     __syncthreads();
-    for (int row = warp; row < cnt; row += 4) {
+    for (int row = warp; warp < nrw && row < cnt; row += nrw) {
       const int nn = s_req[row];
       bool fb = s_kept[row] != 0;
       const int slot = s0 + row;
@@ -797,9 +835,28 @@ bool tile_search_supported(int d, int k, int margin) {
 
 // Shared memory of one CTA for a per-query buffer of `cap` entries.
 static size_t tile_smem_bytes(int KD, int cap) {
-  return tc::tile_bytes(kTM, KD) + tc::tile_bytes(kTN, KD) + (size_t)KD * 4 +
-         (size_t)kTN * 16 + 11 * (size_t)kTN * 4 + (4 + 4) * 4 + 4 * 256 * 4 + 8 + 4 + 16 + 16 +
-         4 * (size_t)cap * 12 + 4 * (size_t)(KD / 4) * 16;
+  return tiles_bytes(KD) + (size_t)KD * 4 + (size_t)kTN * 16 + 11 * (size_t)kTN * 4 +
+         (size_t)(2 * kTM / 32 + 4) * 4 + 4 * 256 * 4 + 8 + 4 + 16 + 16 + 4 * (size_t)cap * 12 +
+         4 * (size_t)(KD / 4) * 16;
+}
+
+// Threads per CTA: 2 kTM where the re-ranking state of four more warps fits
+// the tile region (dp4 <= KD / 4), kTM otherwise.
+static int tile_threads(int KD, int cap) {
+  const size_t wstate = (size_t)cap * 12 + (size_t)(KD / 4) * 16 + 256 * 4;
+  return 4 * wstate <= tiles_bytes(KD) ? 2 * kTM : kTM;
+}
+
+template <int NT>
+static int set_tile_attributes(size_t smem) {
+  KNN_CUDA_TRY(cudaFuncSetAttribute(tile_search_kernel<NT>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // the whole unified L1 as shared memory: the CTAs per SM are then set by
+  // shared memory alone (the default split allowed one)
+  KNN_CUDA_TRY(cudaFuncSetAttribute(tile_search_kernel<NT>,
+                                    cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    cudaSharedmemCarveoutMaxShared));
+  return KNN_OK;
 }
 
 int tile_search_geometry(int d, int k, int margin, int num_sms, int *grid, int *cap, int *P,
@@ -813,20 +870,17 @@ int tile_search_geometry(int d, int k, int margin, int num_sms, int *grid, int *
   // at least 48 KB: no more than four CTAs (4 x 128 TMEM columns) per SM
   *smem = std::max<size_t>(tile_smem_bytes(KD, *cap), 48 * 1024 + 1024);
   if (*smem > 227 * 1024) return KNN_EINVAL;
-  KNN_CUDA_TRY(cudaFuncSetAttribute(tile_search_kernel,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
-  // the whole unified L1 as shared memory: the CTAs per SM are then set by
-  // shared memory alone (the default split allowed one)
-  KNN_CUDA_TRY(cudaFuncSetAttribute(tile_search_kernel,
-                                    cudaFuncAttributePreferredSharedMemoryCarveout,
-                                    cudaSharedmemCarveoutMaxShared));
+  const int nt = tile_threads(KD, *cap);
+  const int rc = nt == kTM ? set_tile_attributes<kTM>(*smem) : set_tile_attributes<2 * kTM>(*smem);
+  if (rc != KNN_OK) return rc;
   // CTAs per SM by shared memory (1 KB of it reserved per CTA); the
   // persistent CTAs that find no SM slot simply start later
   int dev = 0, smem_sm = 0;
   KNN_CUDA_TRY(cudaGetDevice(&dev));
   KNN_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
   int per_sm = (int)((size_t)smem_sm / (*smem + 1024));
-  per_sm = std::max(1, std::min(per_sm, 4));
+  // and by registers: 128 per thread, so four CTAs of kTM threads, two of 2 kTM
+  per_sm = std::max(1, std::min(per_sm, nt == kTM ? 4 : 2));
   *grid = num_sms * per_sm;
   return KNN_OK;
 }
@@ -839,7 +893,10 @@ int launch_tile_list(const int32_t *qoff, int Rq, int c_base, int32_t *tiles, in
 }
 
 int launch_tile_search(const TileArgs &a, int grid, size_t smem, cudaStream_t s) {
-  tile_search_kernel<<<grid, kTM, smem, s>>>(a);
+  if (tile_threads(a.KD, a.cap) == kTM)
+    tile_search_kernel<kTM><<<grid, kTM, smem, s>>>(a);
+  else
+    tile_search_kernel<2 * kTM><<<grid, 2 * kTM, smem, s>>>(a);
   KNN_LAUNCH_CHECK();
   return KNN_OK;
 }
