@@ -600,10 +600,9 @@ def form_c2(torch, dev, flush, steps):
     r, q = data.config2()
     k = 32
     forms, same = _pair_forms(torch, dev, flush, r, q, k,
-                              dict(qreps=1000, sreps=1000, lloyd_iters=3, rep_trials=1), steps,
-                              1000, 22)
+                              dict(qreps=1000, sreps=1000, lloyd_iters=3), steps, 1000, 22)
     return {"workload": f"N={r.shape[0]} M={q.shape[0]} d=32 k={k} reps 1000/1000 lloyd 3, "
-                        "1 draw trial, synthetic 1,000-Gaussian mixture",
+                        "10 draw trials, synthetic 1,000-Gaussian mixture",
             "fp32": forms["fp32"], "bf16_refine": forms["bf16_refine"],
             "same_neighbor_sets": same,
             "bf16_over_fp32": forms["bf16_refine"]["queries_per_s"] / forms["fp32"]["queries_per_s"]}
