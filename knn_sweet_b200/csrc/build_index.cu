@@ -128,7 +128,8 @@ __global__ void __launch_bounds__(256)
 
 // Picks the first trial whose score, compared as float against a running
 // best starting at 0.0f, is larger (selectReps_max, knnjoin.cu:135-148) and
-// gathers its rows.  One block.
+// gathers its rows.  Every block picks the trial (a few hundred scores at
+// most) and copies a slice of the rows.
 __global__ void rep_pick_kernel(const float4 *__restrict__ rows, int dp4,
                                 const int32_t *__restrict__ cand, int R,
                                 int trials, const uint32_t *__restrict__ score,
@@ -149,10 +150,13 @@ __global__ void rep_pick_kernel(const float4 *__restrict__ rows, int dp4,
   }
   __syncthreads();
   const int32_t *c = cand + (int64_t)best_s * R;
-  for (int i = threadIdx.x; i < R; i += blockDim.x) {
-    int32_t row = c[i];
-    if (rep_rows) rep_rows[i] = row;
-    for (int k = 0; k < dp4; k++) reps[(int64_t)i * dp4 + k] = rows[(int64_t)row * dp4 + k];
+  const int64_t total = (int64_t)R * dp4;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e / dp4), kk = (int)(e - (int64_t)i * dp4);
+    const int32_t row = c[i];
+    if (kk == 0 && rep_rows) rep_rows[i] = row;
+    reps[e] = rows[(int64_t)row * dp4 + kk];
   }
 }
 
@@ -641,14 +645,19 @@ int launch_rep_select(const float4 *rows, int dp4, const int32_t *cand_dev,
                       int R, int trials, uint32_t *score_dev, float4 *reps,
                       int32_t *rep_rows, cudaStream_t s) {
   KNN_CUDA_TRY(cudaMemsetAsync(score_dev, 0, sizeof(uint32_t) * trials, s));
-  // 4 x 4 pairs per thread: 8 x 8 (fewer shared-memory loads per fma) took
-  // about 160 registers and measured slower on 8,192 representatives
-  const int nb = (R + 63) / 64;
-  dim3 grid((unsigned)(nb * (nb + 1) / 2), 1, trials);
-  rep_score_kernel<4><<<grid, 256, 0, s>>>(rows, dp4, cand_dev, R, score_dev);
-  KNN_LAUNCH_CHECK();
-  rep_pick_kernel<<<1, 256, 0, s>>>(rows, dp4, cand_dev, R, trials, score_dev,
-                                    reps, rep_rows);
+  // a single draw needs no score (the pick keeps trial 0 either way)
+  if (trials > 1) {
+    // 4 x 4 pairs per thread: 8 x 8 (fewer shared-memory loads per fma) took
+    // about 160 registers and measured slower on 8,192 representatives
+    const int nb = (R + 63) / 64;
+    dim3 grid((unsigned)(nb * (nb + 1) / 2), 1, trials);
+    rep_score_kernel<4><<<grid, 256, 0, s>>>(rows, dp4, cand_dev, R, score_dev);
+    KNN_LAUNCH_CHECK();
+  }
+  const int64_t words = (int64_t)R * dp4;
+  const int pick_blocks = (int)std::min<int64_t>(1024, std::max<int64_t>(1, (words + 255) / 256));
+  rep_pick_kernel<<<pick_blocks, 256, 0, s>>>(rows, dp4, cand_dev, R, trials, score_dev, reps,
+                                              rep_rows);
   KNN_LAUNCH_CHECK();
   return KNN_OK;
 }

@@ -5,7 +5,7 @@
 
   c1        skin-like self-join, N = M = 245,057, d = 3, k = 200, reps 800/800
   c2        N = 1,000,000, M = 100,000, d = 32, k = 32, reps 1000/1000, 3 refinement steps
-  c3        N = 2,000,000, M = 200,000, d = 128, k = 100, reps 8192/8192, 4 steps
+  c3        N = 2,000,000, M = 200,000, d = 128, k = 100, reps 8192/8192, 4 steps, 1 draw
   c3-small  N = 400,000, M = 40,000, d = 128, k = 100, reps 1600/1600, 4 steps (sized
             for profiler captures: inputs above L2, a few hundred MB on the device)
   c4        4,096 ellipsoid clouds (256..16,384 points), d = 3, per-cloud self-join, k = 16
@@ -54,7 +54,8 @@ def main(argv=None):
         _pair_join("c2", q, r, 32, a.form, a.repeat, qreps=1000, sreps=1000, lloyd_iters=3)
     elif a.workload == "c3":
         r, q = data.config3()
-        _pair_join("c3", q, r, 100, a.form, a.repeat, qreps=8192, sreps=8192, lloyd_iters=4)
+        _pair_join("c3", q, r, 100, a.form, a.repeat, qreps=8192, sreps=8192, lloyd_iters=4,
+                   rep_trials=1)
     elif a.workload == "c3-small":
         r, q = data.gaussian_mix(400_000, 40_000, 128, 800, seed=3, center_kind="normal3",
                                  sigma=0.5)
