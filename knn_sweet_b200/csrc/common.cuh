@@ -140,6 +140,26 @@ __device__ __forceinline__ int warp_lower_bound(const float *__restrict__ a,
   return lo + __popc(__ballot_sync(kFull, lt));
 }
 
+// A start for a walk up a sorted array towards the first a[i] >= v: a
+// position lo with a[i] < v for every i < lo and that first element at most
+// 31 places further on.  The 32-ary search of warp_lower_bound without its
+// last level, which saves a dependent load round trip; the walk's own range
+// test skips the few elements below v.
+__device__ __forceinline__ int warp_lower_bound_coarse(const float *__restrict__ a, int n,
+                                                       float v, int lane) {
+  int lo = 0, hi = n;
+  while (hi - lo > 32) {
+    const int step = (hi - lo + 31) >> 5;
+    const int p = lo + (lane + 1) * step - 1;
+    const int c = __popc(__ballot_sync(kFull, (p < hi) && (a[p] < v)));
+    if (step <= 32) return lo + c * step;
+    const int nhi = lo + (c + 1) * step - 1;
+    lo += c * step;
+    hi = nhi < hi ? nhi : hi;
+  }
+  return lo;
+}
+
 // Per-thread last-error text (the C ABI never exits the process).
 void set_error(const char *fmt, ...);
 std::string &error_buffer();

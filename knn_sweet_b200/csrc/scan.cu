@@ -205,6 +205,12 @@ __device__ __forceinline__ void smem_bitonic_sort(uint64_t *s, int lane) {
 #ifndef KNN_TOPK_EARLY
 #define KNN_TOPK_EARLY 160
 #endif
+// Mid-query compactions keep every key up to band_hi of an upper bound of the
+// k-th distance from one linear-bin histogram pass (1) or of the exact k-th
+// from the radix selection (0).
+#ifndef KNN_LINEAR_SELECT
+#define KNN_LINEAR_SELECT 1
+#endif
 
 template <int LL>
 struct SelectTopK : TopKBase {
@@ -268,8 +274,14 @@ struct SelectTopK : TopKBase {
   __device__ __forceinline__ void make_room(int lane, int d) {
     if (nbuf <= k) return;
     __syncwarp();
+#if KNN_LINEAR_SELECT
+    // an upper bound of the k-th: the threshold it gives admits a little more
+    const uint32_t T = warp_kth_upper_u32(reinterpret_cast<const uint32_t *>(buf) + 1, 2,
+                                          nbuf, k, hist, lane);
+#else
     const uint32_t T = warp_select_kth_u32(reinterpret_cast<const uint32_t *>(buf) + 1, 2,
                                            nbuf, k, hist, lane);
+#endif
     const uint32_t W = __float_as_uint(band_hi(__uint_as_float(T), d));
     int w = 0;
     for (int b0 = 0; b0 < nbuf; b0 += 32) {
@@ -553,6 +565,13 @@ struct QueryRow<0, IDXROW> {
 #ifndef KNN_WALK_OUTWARD
 #define KNN_WALK_OUTWARD 0
 #endif
+// Visits take a cluster's bounds and member range from the lanes that tested
+// it (loaded once per batch of 32 candidate clusters) and start the band
+// walk from the coarse member search (1); or reload them per visit and
+// search to the exact band edge (0).
+#ifndef KNN_VISIT_META
+#define KNN_VISIT_META 1
+#endif
 
 // Largest k kept in a register list (one key per lane): up to 24, so that
 // 8 of the 32 slots or more hold the FP32 band behind the k-th; larger k use
@@ -662,12 +681,26 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
       int rs = 0;
       float D = 0.0f;
       bool alive = false;
+#if KNN_VISIT_META
+      float cmx = 0.0f, cmn = 0.0f;
+      int cst = 0, cnn = 0;
+#endif
       if (j < nr) {
         rs = rl[j];
         D = sqrtf(qr.dist2(a.sreps + (int64_t)rs * dp4, dp4));
         const float th = tk.theta;
         const float slack = tol * (2.0f * D + 2.0f * th);
+#if KNN_VISIT_META
+        cmx = a.cmax[rs];
+        cmn = a.cmin[rs];
+        alive = !(D - cmx > th + slack) && !(D + th + slack < cmn);
+        if (alive) {
+          cst = a.soff[rs];
+          cnn = a.soff[rs + 1] - cst;
+        }
+#else
         alive = !(D - a.cmax[rs] > th + slack) && !(D + th + slack < a.cmin[rs]);
+#endif
         if (!alive) pruned++;
       }
       // visit this chunk's surviving clusters: in list order (by rep-rep
@@ -725,16 +758,27 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
           amask &= ~(1u << src);
         }
         const float Dc = __shfl_sync(kFull, D, src);
+#if KNN_VISIT_META
+        const float cmax_c = __shfl_sync(kFull, cmx, src);
+        const float cmin_c = __shfl_sync(kFull, cmn, src);
+#else
         const int c = __shfl_sync(kFull, rs, src);
+        const float cmax_c = a.cmax[c], cmin_c = a.cmin[c];
+#endif
         float th = tk.theta;
         float slack = tol * (2.0f * Dc + 2.0f * th);
-        if (Dc - a.cmax[c] > th + slack || Dc + th + slack < a.cmin[c]) {
+        if (Dc - cmax_c > th + slack || Dc + th + slack < cmin_c) {
           if (lane == 0) pruned++;
           continue;
         }
         if (lane == 0) visited++;
+#if KNN_VISIT_META
+        const int start = __shfl_sync(kFull, cst, src);
+        const int n_c = __shfl_sync(kFull, cnn, src);
+#else
         const int start = a.soff[c];
         const int n_c = a.soff[c + 1] - start;
+#endif
 #if KNN_WALK_OUTWARD
         // members below `mid` have d(s,Rs) < Dc, from `mid` on >= Dc; walk
         // outward from there, alternately up and down
@@ -769,7 +813,11 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
         // one direction: from the lower band edge up (no search when the band
         // starts below the cluster's nearest member)
         const float lo_edge = Dc - th - slack;
-        const int lo = lo_edge <= a.cmin[c] ? 0 : warp_lower_bound(a.sdist + start, n_c, lo_edge, lane);
+#if KNN_VISIT_META
+        const int lo = lo_edge <= cmin_c ? 0 : warp_lower_bound_coarse(a.sdist + start, n_c, lo_edge, lane);
+#else
+        const int lo = lo_edge <= cmin_c ? 0 : warp_lower_bound(a.sdist + start, n_c, lo_edge, lane);
+#endif
         for (int p0 = lo; p0 < n_c; p0 += 32) {
           th = tk.theta;
           slack = tol * (2.0f * Dc + 2.0f * th);

@@ -165,6 +165,63 @@ __device__ __forceinline__ uint32_t warp_select_kth_u32(const uint32_t *s, int s
   return prefix | (vand & ((1u << lb) - 1u));  // the common low bits
 }
 
+// An upper bound of the k-th smallest (1-based, 1 <= k <= n) of the
+// non-negative floats s[i * stride], i < n (as bit patterns), that is itself
+// one of the values: the largest value of the bin holding the k-th, the bins
+// splitting [min, max] into 128 equal parts.  bin(v) is non-decreasing in v
+// (subtraction, multiplication by a positive factor and truncation all are),
+// so the values of the bins up to that bin are the smallest ones and the k-th
+// lies among them.  One min / max pass and one histogram pass (counts and
+// per-bin maxima, `hist`: 256 shared words), against two to four passes of
+// the exact radix selection; for a pruning threshold an upper bound is as
+// good as the k-th itself.
+__device__ __forceinline__ uint32_t warp_kth_upper_u32(const uint32_t *s, int stride, int n,
+                                                       int k, uint32_t *hist, int lane) {
+  uint32_t mn = 0xffffffffu, mx = 0u;
+  for (int i = lane; i < n; i += 32) {
+    const uint32_t v = s[(size_t)i * stride];
+    mn = min(mn, v);
+    mx = max(mx, v);
+  }
+  mn = __reduce_min_sync(kFull, mn);
+  mx = __reduce_max_sync(kFull, mx);
+  if (mn == mx) return mx;
+  const float fmn = __uint_as_float(mn);
+  const float scale = fminf(128.0f / (__uint_as_float(mx) - fmn), 1e30f);
+  __syncwarp();
+#pragma unroll
+  for (int b = 0; b < 8; b++) hist[b * 32 + lane] = 0;
+  __syncwarp();
+  for (int i = lane; i < n; i += 32) {
+    const uint32_t v = s[(size_t)i * stride];
+    const int b = min((int)((__uint_as_float(v) - fmn) * scale), 127);
+    atomicAdd(&hist[b], 1u);
+    atomicMax(&hist[128 + b], v);
+  }
+  __syncwarp();
+  uint32_t base = 0;
+  int bin = 127;
+#pragma unroll 1
+  for (int j = 0; j < 4; j++) {
+    const uint32_t h = hist[j * 32 + lane];
+    uint32_t incl = h;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    if (base + total >= (uint32_t)k) {
+      bin = j * 32 + __ffs(__ballot_sync(kFull, base + incl >= (uint32_t)k)) - 1;
+      break;
+    }
+    base += total;
+  }
+  const uint32_t r = hist[128 + bin];
+  __syncwarp();
+  return r;
+}
+
 // ---------------------------------------------------------------------------
 // Register bitonic networks over 32*E keys, blocked layout: lane l holds
 // positions E*l .. E*l+E-1.  Strides >= E pair registers of different lanes
