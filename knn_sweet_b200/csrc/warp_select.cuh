@@ -222,6 +222,87 @@ __device__ __forceinline__ uint32_t warp_kth_upper_u32(const uint32_t *s, int st
   return r;
 }
 
+// Sorts the n <= 32*E distinct keys s[0..n) ascending, by one warp, in three
+// passes instead of a bitonic network: the keys are counted into 128 linear
+// bins of their distance words between the smallest and the largest (bin(v)
+// non-decreasing in v, so bins hold consecutive runs of the sorted order), an
+// exclusive scan gives every bin its first position, the keys are placed bin
+// by bin into tmp (n keys of scratch), and every key then moves to its bin's
+// first position plus its rank among the keys of its bin.  Returns false,
+// having changed nothing, when a bin holds more than kMaxBin keys (many equal
+// distances: the rank loop would cost more than the network).  `hist`: 256
+// shared words.
+template <int E>
+__device__ __forceinline__ bool warp_bin_sort(uint64_t *s, int n, uint64_t *tmp,
+                                              uint32_t *hist, int lane) {
+  constexpr uint32_t kMaxBin = 48;
+  uint32_t mn = 0xffffffffu, mx = 0u;
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    const int i = j * 32 + lane;
+    if (i < n) {
+      const uint32_t v = (uint32_t)(s[i] >> 32);
+      mn = min(mn, v);
+      mx = max(mx, v);
+    }
+  }
+  mn = __reduce_min_sync(kFull, mn);
+  mx = __reduce_max_sync(kFull, mx);
+  const float fmn = __uint_as_float(mn);
+  const float scale = mx > mn ? fminf(128.0f / (__uint_as_float(mx) - fmn), 1e30f) : 0.0f;
+  __syncwarp();
+#pragma unroll
+  for (int b = 0; b < 4; b++) hist[b * 32 + lane] = 0;
+  __syncwarp();
+  uint32_t tag[E];  // bin << 16 | place inside the bin
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    const int i = j * 32 + lane;
+    tag[j] = 0;
+    if (i < n) {
+      const float v = __uint_as_float((uint32_t)(s[i] >> 32));
+      const uint32_t b = (uint32_t)min((int)((v - fmn) * scale), 127);
+      tag[j] = (b << 16) | atomicAdd(&hist[b], 1u);
+    }
+  }
+  __syncwarp();
+  uint32_t base = 0, big = 0;
+#pragma unroll
+  for (int jj = 0; jj < 4; jj++) {
+    const uint32_t h = hist[jj * 32 + lane];
+    big = max(big, h);
+    uint32_t incl = h;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
+    }
+    hist[128 + jj * 32 + lane] = base + incl - h;
+    base += __shfl_sync(kFull, incl, 31);
+  }
+  if (__reduce_max_sync(kFull, big) > kMaxBin) return false;
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    const int i = j * 32 + lane;
+    if (i < n) tmp[hist[128 + (tag[j] >> 16)] + (tag[j] & 0xffffu)] = s[i];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < E; j++) {
+    const int i = j * 32 + lane;
+    if (i < n) {
+      const uint32_t b = tag[j] >> 16, st = hist[128 + b], cnt = hist[b];
+      const uint64_t key = tmp[st + (tag[j] & 0xffffu)];
+      uint32_t r = 0;
+      for (uint32_t t = 0; t < cnt; t++) r += tmp[st + t] < key;
+      s[st + r] = key;
+    }
+  }
+  __syncwarp();
+  return true;
+}
+
 // ---------------------------------------------------------------------------
 // Register bitonic networks over 32*E keys, blocked layout: lane l holds
 // positions E*l .. E*l+E-1.  Strides >= E pair registers of different lanes
