@@ -205,17 +205,6 @@ __device__ __forceinline__ void smem_bitonic_sort(uint64_t *s, int lane) {
 #ifndef KNN_TOPK_EARLY
 #define KNN_TOPK_EARLY 160
 #endif
-// Mid-query compactions keep every key up to band_hi of an upper bound of the
-// k-th distance from one linear-bin histogram pass (1) or of the exact k-th
-// from the radix selection (0).
-#ifndef KNN_LINEAR_SELECT
-#define KNN_LINEAR_SELECT 1
-#endif
-// End-of-query sort of more than 128 candidates: binned counting sort (1) or
-// the shared-memory bitonic network (0).
-#ifndef KNN_BIN_SORT
-#define KNN_BIN_SORT 1
-#endif
 
 template <int LL>
 struct SelectTopK : TopKBase {
@@ -351,20 +340,22 @@ struct SelectTopK : TopKBase {
   }
 };
 
-// Offer one key per lane (kKeyMax = nothing); warp-collective.
+// Offer one candidate per lane, warp-collective: the lanes with `pass` set
+// (squared distance v at most the threshold's distance word, so that the key
+// (v, idx) lies below the threshold key) append their keys.
 template <class TK>
-__device__ __forceinline__ void topk_push(TK &tk, uint64_t key, int lane, int d) {
-  bool pass = key < tk.thr;
+__device__ __forceinline__ void topk_offer(TK &tk, bool pass, float v, int32_t idx, int lane,
+                                           int d) {
   unsigned b = __ballot_sync(kFull, pass);
   if (b == 0) return;
   int cnt = __popc(b);
   if (tk.nbuf + cnt > tk.cap()) {
     tk.make_room(lane, d);
-    pass = key < tk.thr;
+    pass = pass && v <= key_d2(tk.thr);
     b = __ballot_sync(kFull, pass);
     cnt = __popc(b);
   }
-  if (pass) tk.buf[tk.nbuf + __popc(b & ((1u << lane) - 1))] = key;
+  if (pass) tk.buf[tk.nbuf + __popc(b & ((1u << lane) - 1))] = make_key(v, idx);
   tk.nbuf += cnt;
   tk.pushed += cnt;
 }
@@ -673,15 +664,13 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
         inb = valid && dsv >= lo_v && dsv <= hi_v;
         if (inb) v = qr.dist2(a.srows + gp * dp4, dp4);
       }
-      uint64_t key = kKeyMax;
+      bool pass = false;
       if (inb) {
         evals++;
-        if (v <= key_d2(tk.thr)) {
-          if (!IDXROW) idx = a.sidx[gp];
-          key = make_key(v, idx);
-        }
+        pass = v <= key_d2(tk.thr);
+        if (!IDXROW && pass) idx = a.sidx[gp];
       }
-      topk_push(tk, key, lane, a.d);
+      topk_offer(tk, pass, v, idx, lane, a.d);
       return dsv;
     };
 

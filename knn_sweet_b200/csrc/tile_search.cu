@@ -182,13 +182,18 @@ __device__ __forceinline__ void stage_tile(unsigned char *tile, const float *sc,
 }
 
 // Keeps the entries of a bound buffer (lu, pos: n entries in shared memory)
-// whose lower bound is at most the k-th smallest upper bound -- no entry
-// beyond it can be among the k nearest; in place, by one warp.  Returns the
-// count kept and that bound.  Needs n >= k.
+// whose lower bound is at most the k-th smallest upper bound, or an upper
+// bound of it -- no entry beyond it can be among the k nearest; in place, by
+// one warp.  Returns the count kept and that bound.  Needs n >= k.
 __device__ __forceinline__ int compact_bounds(float2 *lu, int32_t *pos, int n, int k,
                                               uint32_t *hist, int lane, float *uk_out) {
+#if KNN_LINEAR_SELECT
+  const float uk = __uint_as_float(
+      warp_kth_upper_u32(reinterpret_cast<const uint32_t *>(lu) + 1, 2, n, k, hist, lane));
+#else
   const float uk = __uint_as_float(
       warp_select_kth_u32(reinterpret_cast<const uint32_t *>(lu) + 1, 2, n, k, hist, lane));
+#endif
   int w = 0;
   for (int b0 = 0; b0 < n; b0 += 32) {
     const int i = b0 + lane;
@@ -716,8 +721,14 @@ __global__ void __launch_bounds__(NT, NT == kTM ? 4 : 2)
           m2 = w;
         }
       } else if (!fb && m1 > k) {
-        const uint64_t kth = warp_select_kth(keys, m1, k, whist, lane);
-        const float Dk = key_d2(kth);
+        // keys up to band_hi of (an upper bound of) the k-th; the band itself
+        // is settled on the sorted keys below
+#if KNN_LINEAR_SELECT
+        const float Dk = __uint_as_float(warp_kth_upper_u32(
+            reinterpret_cast<const uint32_t *>(keys) + 1, 2, m1, k, whist, lane));
+#else
+        const float Dk = key_d2(warp_select_kth(keys, m1, k, whist, lane));
+#endif
         const float lim2 = band_hi(Dk, d);
         int w = 0;
         for (int b0 = 0; b0 < m1; b0 += 32) {
@@ -737,9 +748,16 @@ __global__ void __launch_bounds__(NT, NT == kTM ? 4 : 2)
       if (!fb && np2 > cap) fb = true;
       if (!fb) {
         if (!sorted) {
-          for (int e = m2 + lane; e < np2; e += 32) keys[e] = kKeyMax;
-          __syncwarp();
-          smem_bitonic_sort_rt(keys, np2, lane);
+#if KNN_BIN_SORT
+          // binned counting sort where its scratch fits behind the keys
+          sorted = m2 <= 256 && np2 + m2 <= cap &&
+                   warp_bin_sort<8>(keys, m2, keys + np2, whist, lane);
+#endif
+          if (!sorted) {
+            for (int e = m2 + lane; e < np2; e += 32) keys[e] = kKeyMax;
+            __syncwarp();
+            smem_bitonic_sort_rt(keys, np2, lane);
+          }
         }
         if (m2 > k) {
           // keys at or above Dk - band were ranked in FP32 only to within

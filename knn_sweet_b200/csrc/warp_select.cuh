@@ -6,6 +6,19 @@
 
 #include "common.cuh"
 
+// Compactions that only need a pruning threshold (the scan's mid-query
+// candidate set, the tile search's bound buffer) select an upper bound of the
+// k-th value from one linear-bin histogram pass (1) or the exact k-th by
+// radix selection (0).
+#ifndef KNN_LINEAR_SELECT
+#define KNN_LINEAR_SELECT 1
+#endif
+// Final sorts of 129 to 256 candidate keys: binned counting sort (1) or the
+// shared-memory bitonic network (0).
+#ifndef KNN_BIN_SORT
+#define KNN_BIN_SORT 1
+#endif
+
 namespace knnsweet {
 
 __device__ __forceinline__ uint64_t shfl_xor64(uint64_t v, int m) {
