@@ -14,19 +14,17 @@
 //     on D), so the running k-th distance theta falls early.
 //   - Members are stored contiguously, ascending by d(s, Rs).  Members within
 //     theta of q satisfy |D - d(s,Rs)| <= theta (knnjoin.cu:796-801), a
-//     contiguous band around the member whose d(s,Rs) is closest to D.  A
-//     warp-wide 32-ary search finds that member; the warp then walks outward,
-//     32 members per step, alternately up and down, with coalesced row loads,
-//     and stops in each direction at the first step that leaves the band
-//     (re-evaluated with the current theta).
-//   - Exact FP32 distances go through the warp top-k: candidates whose
-//     (d^2, index) key beats the current k-th key are appended to a
-//     shared-memory buffer; a full buffer is sorted and merged into the sorted
-//     list of the k best, after which theta is the new k-th distance.  For
-//     k <= 256 the list lives in registers (8 keys per lane at most) and the
-//     sort/merge runs on warp shuffles; above 256 both live in shared memory.
-//     This replaces the per-thread insertion into an 8 KB local-memory array
-//     (knnjoin.cu:774, 813-845).
+//     contiguous band.  A warp-wide 32-ary search finds (to within 31
+//     members) where the band starts; the warp walks it 32 members per step
+//     with coalesced row loads and stops at the first step past its upper
+//     end (re-evaluated with the current theta).
+//   - Exact FP32 distances go through the warp top-k: k <= 24 a sorted
+//     register list (one key per lane) merged by shuffle networks; larger k
+//     an unsorted candidate set in shared memory, compacted to the keys up to
+//     the FP32 band of (an upper bound of) the k-th distance when it fills,
+//     sorted once at the end of the query.  This replaces the per-thread
+//     insertion into an 8 KB local-memory array (knnjoin.cu:774, 813-845).
+//   - The k-th boundary is then settled in FP64 (see TopKBase).
 // Bounds are widened by a rounding slack (bound_tol) so that FP32 rounding
 // never prunes a point that the FP32 distances would rank in the top k.
 #include <type_traits>

@@ -62,6 +62,31 @@ def test_float_dims(cuda_device, oracle, d, k):
     assert_matches(idx, dist, oi, od, exact=False)
 
 
+@pytest.mark.parametrize("k", [129, 200, 256])
+def test_float_candidate_set_sorts(cuda_device, oracle, k):
+    # k in 129..256: the shared-memory candidate set, compacted by the
+    # linear-bin bound of the k-th and sorted at the end by the binned
+    # counting sort (float distances: few equal values per bin)
+    r, q = data.gaussian_mix(30000, 800, 3, 20, seed=300 + k)
+    idx, dist, st = knnjoin(q, r, k, qreps=60, sreps=60, stats=True)
+    oi, od = oracle.bruteforce_f64(q, r, k)
+    assert_matches(idx, dist, oi, od)
+    assert np.all(np.diff(dist, axis=1) >= 0)
+    assert st.topk_merges > 0
+
+
+def test_crowded_bins_take_the_network(cuda_device, oracle):
+    # integer points on a small grid: hundreds of candidates share each
+    # squared distance, more than a bin of the counting sort takes, so the end
+    # of every query sorts by the bitonic network instead
+    rng = np.random.default_rng(11)
+    x = rng.integers(0, 5, size=(20000, 3)).astype(np.float32)
+    rows = np.arange(0, 20000, 97)
+    idx, dist = knnjoin(x, None, 200, qreps=30, sreps=30)
+    oi, od = oracle.bruteforce_f64(x, x, 200, qrows=rows)
+    assert_matches(idx[rows], dist[rows], oi, od, exact=True)
+
+
 def test_cross_join_separate_reps(cuda_device, oracle):
     r = data.skin_like(25000, seed=31)
     q = data.skin_like(4000, seed=32)
@@ -105,10 +130,11 @@ def test_deterministic_and_apis_agree(cuda_device):
         assert np.array_equal(u, v)
 
 
-@pytest.mark.parametrize("m,k", [(60000, 40), (33333, 200)])
+@pytest.mark.parametrize("m,k", [(60000, 40), (33333, 200), (100000, 200)])
 def test_host_path_chunked_copies_match_device_path(cuda_device, m, k):
-    """Large host-buffer joins scan in row chunks and copy each chunk back while
-    the next runs; the result must equal the device-buffer join's."""
+    """Large host-buffer joins scan in row chunks (about 16 MB of results each,
+    8 to 32 chunks: 160 MB here gives 9) and copy each chunk back while the
+    next runs; the result must equal the device-buffer join's."""
     x = data.skin_like(m, seed=61)
     a = knnjoin(x, None, k)
     b = torch_join(x, x, k)
