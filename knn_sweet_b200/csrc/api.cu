@@ -585,6 +585,39 @@ int search_clusters(const RefSide &R, const QuerySide &Q, int64_t m, int32_t k, 
   return KNN_OK;
 }
 
+// Two non-blocking streams of the calling thread on the current device for a
+// host-buffer call (the work and the copy-back), created on first use and
+// kept for the thread's lifetime: creating and destroying them took about a
+// quarter of a millisecond of every call.  Every host-buffer call leaves both
+// idle when it returns.
+int host_streams(cudaStream_t *s, cudaStream_t *cs) {
+  int dev = 0;
+  KNN_CUDA_TRY(cudaGetDevice(&dev));
+  struct Pair {
+    int dev;
+    cudaStream_t s, cs;
+  };
+  thread_local std::vector<Pair> cache;
+  for (const Pair &p : cache)
+    if (p.dev == dev) {
+      *s = p.s;
+      *cs = p.cs;
+      return KNN_OK;
+    }
+  Pair p{dev, nullptr, nullptr};
+  KNN_CUDA_TRY(cudaStreamCreateWithFlags(&p.s, cudaStreamNonBlocking));
+  if (cudaStreamCreateWithFlags(&p.cs, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    cudaStreamDestroy(p.s);
+    set_error("stream creation failed");
+    return KNN_ECUDA;
+  }
+  cache.push_back(p);
+  *s = p.s;
+  *cs = p.cs;
+  return KNN_OK;
+}
+
 // Copies the device counters of one call into `st` (synchronises `s`).
 int read_stats(const unsigned long long *ctr, cudaStream_t s, knn_stats *st) {
   unsigned long long h[kCtrCount];
@@ -821,12 +854,9 @@ int knn_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d,
     return KNN_EINVAL;
   }
   cudaStream_t s, cs;
-  KNN_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
-    cudaGetLastError();
-    cudaStreamDestroy(s);
-    set_error("stream creation failed");
-    return KNN_ECUDA;
+  {
+    const int rc = host_streams(&s, &cs);
+    if (rc != KNN_OK) return rc;
   }
   int rc = KNN_OK;
   HostSink sink{out_idx, out_dist, cs, false};
@@ -878,8 +908,6 @@ int knn_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d,
     set_error("join failed on the device: %s", cudaGetErrorString(e));
     rc = KNN_ECUDA;
   }
-  cudaStreamDestroy(cs);
-  cudaStreamDestroy(s);
   return rc;
 }
 

@@ -793,8 +793,11 @@ extern "C" int knn_join_batched(const float *q, const int64_t *q_offsets, const 
     return KNN_EINVAL;
   }
   const bool self = q == r && std::equal(q_offsets, q_offsets + ncloud + 1, r_offsets);
-  cudaStream_t s;
-  KNN_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  cudaStream_t s, cs;
+  {
+    const int rc = host_streams(&s, &cs);
+    if (rc != KNN_OK) return rc;
+  }
   int rc = KNN_OK;
   {
     BatchArena ar(s);
@@ -831,6 +834,5 @@ extern "C" int knn_join_batched(const float *q, const int64_t *q_offsets, const 
     set_error("batched join failed on the device: %s", cudaGetErrorString(e));
     rc = KNN_ECUDA;
   }
-  cudaStreamDestroy(s);
   return rc;
 }

@@ -150,4 +150,8 @@ int launch_tile_list(const int32_t *qoff, int Rq, int c_base, int32_t *tiles, in
                      cudaStream_t s);
 int launch_tile_search(const TileArgs &a, int grid, size_t smem, cudaStream_t s);
 
+// The calling thread's two streams for host-buffer calls (cached per device,
+// idle between calls).
+int host_streams(cudaStream_t *s, cudaStream_t *cs);
+
 }  // namespace knnsweet

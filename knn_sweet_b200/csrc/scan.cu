@@ -573,6 +573,10 @@ struct QueryRow<0, IDXROW> {
 #define KNN_VISIT_META 1
 #endif
 
+#ifndef KNN_INDEX32
+#define KNN_INDEX32 1
+#endif
+
 // Largest k kept in a register list (one key per lane): up to 24, so that
 // 8 of the 32 slots or more hold the FP32 band behind the k-th; larger k use
 // the shared-memory candidate set.
@@ -634,7 +638,13 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
     // one band step: lane's member p of the cluster at `start`, kept when
     // its distance to the representative lies in [lo_v, hi_v]
     auto step = [&](int start, int p, bool valid, float lo_v, float hi_v) -> float {
+#if KNN_INDEX32
+      // row indices fit 32 bits (the result indices are int32): unsigned
+      // offsets make every address one wide multiply-add
+      const unsigned gp = (unsigned)(start + p);
+#else
       const int64_t gp = (int64_t)start + p;
+#endif
       float dsv = 0.0f, v = 0.0f;
       int32_t idx = 0;
       bool inb;
@@ -643,7 +653,7 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
         float4 row[DP4];
         if (valid) {
 #pragma unroll
-          for (int c = 0; c < DP4; c++) row[c] = a.srows[gp * DP4 + c];
+          for (int c = 0; c < DP4; c++) row[c] = a.srows[(size_t)gp * DP4 + c];
           dsv = a.sdist[gp];
         }
         inb = valid && dsv >= lo_v && dsv <= hi_v;
@@ -654,13 +664,13 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
         if (inb) {
           float4 row[DP4];
 #pragma unroll
-          for (int c = 0; c < DP4; c++) row[c] = a.srows[gp * DP4 + c];
+          for (int c = 0; c < DP4; c++) row[c] = a.srows[(size_t)gp * DP4 + c];
           v = qr.dist2_member(row, &idx);
         }
       } else {
         dsv = valid ? a.sdist[gp] : 0.0f;
         inb = valid && dsv >= lo_v && dsv <= hi_v;
-        if (inb) v = qr.dist2(a.srows + gp * dp4, dp4);
+        if (inb) v = qr.dist2(a.srows + (size_t)gp * dp4, dp4);
       }
       bool pass = false;
       if (inb) {
