@@ -23,6 +23,12 @@
 
 #include "common.cuh"
 #include "glibc_rand.h"
+
+// A host-buffer join's first copy-back chunk holds one query per resident
+// scan warp (1), or all chunks are equal (0).
+#ifndef KNN_SMALL_FIRST_CHUNK
+#define KNN_SMALL_FIRST_CHUNK 1
+#endif
 #include "kernels.cuh"
 #include "pipeline.cuh"
 
@@ -253,13 +259,19 @@ struct EventSet {
 
 
 // Events of the chunked copies, destroyed once both streams are idle.
-struct ChunkEvents {
-  std::vector<cudaEvent_t> ev;
-  ~ChunkEvents() {
-    for (auto e : ev)
-      if (e) cudaEventDestroy(e);
+// Events of the chunked copies: the calling thread's, created on first use
+// and reused (a call leaves its streams idle, so the previous call's events
+// have completed).
+int chunk_events(int n, std::vector<cudaEvent_t> **out) {
+  thread_local std::vector<cudaEvent_t> pool;
+  while ((int)pool.size() < n) {
+    cudaEvent_t e;
+    KNN_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    pool.push_back(e);
   }
-};
+  *out = &pool;
+  return KNN_OK;
+}
 
 // Row geometry: float4 chunks per row (rounded up to a power of two for the
 // register-width scan kernels when d <= 32) and the scan template width.
@@ -530,16 +542,30 @@ int search_clusters(const RefSide &R, const QuerySide &Q, int64_t m, int32_t k, 
   // slots still in query-cluster order) and copy every finished chunk back
   // while the next one runs.  About 16 MB of results per chunk, 8 to 32
   // chunks (k = 200 self-join, 392 MB of results: 8.43 ms end to end with 8
-  // chunks, 8.18 with 24, 8.17 with 32; the copy alone takes 6.89 ms)
+  // chunks, 8.18 with 24, 8.17 with 32; the copy alone takes 6.89 ms), the
+  // first one small (8.23 -> 8.10 ms on a box whose copy takes 7.15 ms)
   const int64_t out_bytes = m * (int64_t)k * 8;
   const bool whole = slot0 == 0 && nslot == m;
   const int nchunks =
       (sink && whole && !tiles && out_bytes >= (16 << 20) && m >= 8 * 1024)
           ? (int)std::min<int64_t>(32, std::max<int64_t>(8, out_bytes >> 24))
           : 1;
-  ChunkEvents cev;
   if (nchunks > 1) {
-    const int chunk_rows = (int)((m + nchunks - 1) / nchunks);
+    // the first chunk one query per resident warp of the scan, so that the
+    // copy-back starts after about one query's time; the rest in equal chunks
+    const int64_t first =
+        KNN_SMALL_FIRST_CHUNK ? std::min<int64_t>(m / 4, (int64_t)num_sms * 32) : 0;
+    const int nrest = first > 0 ? nchunks - 1 : nchunks;
+    const int chunk_rows = (int)((m - first + nrest - 1) / nrest);
+    std::vector<int64_t> r0s(nchunks);
+    std::vector<int32_t> counts(nchunks);
+    for (int c = 0; c < nchunks; c++) {
+      const int64_t b = first > 0 ? (c == 0 ? 0 : first + (int64_t)(c - 1) * chunk_rows)
+                                  : (int64_t)c * chunk_rows;
+      const int64_t e = first > 0 && c == 0 ? first : std::min<int64_t>(m, b + chunk_rows);
+      r0s[c] = std::min<int64_t>(b, m);
+      counts[c] = (int32_t)std::max<int64_t>(0, e - r0s[c]);
+    }
     uint32_t *ckeys, *ckeys_out;
     int32_t *cvals, *cslots, *ccount;
     unsigned long long *cwork;
@@ -553,25 +579,22 @@ int search_clusters(const RefSide &R, const QuerySide &Q, int64_t m, int32_t k, 
     KNN_TRY(ar.alloc(&ccount, (size_t)nchunks));
     KNN_TRY(ar.alloc(&cwork, (size_t)nchunks));
     KNN_CUDA_TRY(cudaMemsetAsync(cwork, 0, nchunks * sizeof(unsigned long long), s));
-    std::vector<int32_t> counts(nchunks);
-    for (int c = 0; c < nchunks; c++)
-      counts[c] = (int32_t)std::max<int64_t>(0, std::min<int64_t>(chunk_rows, m - (int64_t)c * chunk_rows));
     KNN_TRY(upload_i32(counts, ccount, s));
-    KNN_TRY(launch_chunk_slots(Q.qset.perm, m, chunk_rows, nchunks, ckeys, ckeys_out, cvals,
-                               cslots, ctemp, tb, s));
-    cev.ev.assign(nchunks, nullptr);
+    KNN_TRY(launch_chunk_slots(Q.qset.perm, m, (int)first, chunk_rows, nchunks, ckeys, ckeys_out,
+                               cvals, cslots, ctemp, tb, s));
+    std::vector<cudaEvent_t> *evs;
+    KNN_TRY(chunk_events(nchunks, &evs));
     for (int c = 0; c < nchunks; c++) {
       if (counts[c] == 0) continue;
-      const int64_t r0 = (int64_t)c * chunk_rows;
+      const int64_t r0 = r0s[c];
       ScanArgs ac = a;
       ac.slot_list = cslots + r0;
       ac.slot_count = reinterpret_cast<const unsigned *>(ccount + c);
       ac.m = counts[c];
       ac.work_counter = cwork + c;
       KNN_TRY(launch_scan(ac, num_sms, s));
-      KNN_CUDA_TRY(cudaEventCreateWithFlags(&cev.ev[c], cudaEventDisableTiming));
-      KNN_CUDA_TRY(cudaEventRecord(cev.ev[c], s));
-      KNN_CUDA_TRY(cudaStreamWaitEvent(sink->copy, cev.ev[c], 0));
+      KNN_CUDA_TRY(cudaEventRecord((*evs)[c], s));
+      KNN_CUDA_TRY(cudaStreamWaitEvent(sink->copy, (*evs)[c], 0));
       const size_t cnt = (size_t)counts[c] * k;
       KNN_CUDA_TRY(cudaMemcpyAsync(sink->idx + r0 * k, out_idx + r0 * k, cnt * sizeof(int32_t),
                                    cudaMemcpyDeviceToHost, sink->copy));

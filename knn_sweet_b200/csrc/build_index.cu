@@ -707,11 +707,14 @@ size_t cluster_sort_temp_bytes(int64_t n, int R) {
 // Query slots grouped by row chunk: chunk c holds the slots of query rows
 // [c * chunk_rows, (c + 1) * chunk_rows), in slot (query-cluster) order -- a
 // stable radix sort of the slots by chunk id.
-__global__ void chunk_keys_kernel(const int32_t *__restrict__ qorder, int64_t m, int chunk_rows,
-                                  uint32_t *__restrict__ keys, int32_t *__restrict__ vals) {
+__global__ void chunk_keys_kernel(const int32_t *__restrict__ qorder, int64_t m, int first,
+                                  int chunk_rows, uint32_t *__restrict__ keys,
+                                  int32_t *__restrict__ vals) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
        i += (int64_t)gridDim.x * blockDim.x) {
-    keys[i] = (uint32_t)(qorder[i] / chunk_rows);
+    const int32_t row = qorder[i];
+    keys[i] = first > 0 ? (row < first ? 0u : 1u + (uint32_t)((row - first) / chunk_rows))
+                        : (uint32_t)(row / chunk_rows);
     vals[i] = (int32_t)i;
   }
 }
@@ -730,10 +733,10 @@ size_t chunk_slots_temp_bytes(int64_t m, int nchunks) {
   return bytes;
 }
 
-int launch_chunk_slots(const int32_t *qorder, int64_t m, int chunk_rows, int nchunks,
+int launch_chunk_slots(const int32_t *qorder, int64_t m, int first, int chunk_rows, int nchunks,
                        uint32_t *keys, uint32_t *keys_out, int32_t *vals, int32_t *slots,
                        void *temp, size_t temp_bytes, cudaStream_t s) {
-  chunk_keys_kernel<<<grid_for(m, 256), 256, 0, s>>>(qorder, m, chunk_rows, keys, vals);
+  chunk_keys_kernel<<<grid_for(m, 256), 256, 0, s>>>(qorder, m, first, chunk_rows, keys, vals);
   KNN_LAUNCH_CHECK();
   KNN_CUDA_TRY(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, keys_out, vals, slots,
                                                (int)m, 0, chunk_bits(nchunks), s));

@@ -87,7 +87,7 @@ int launch_cluster_sort(const int32_t *cl, const float *dr, int64_t n, int R,
                         int32_t *perm, void *temp, size_t temp_bytes,
                         cudaStream_t s);
 size_t chunk_slots_temp_bytes(int64_t m, int nchunks);
-int launch_chunk_slots(const int32_t *qorder, int64_t m, int chunk_rows, int nchunks,
+int launch_chunk_slots(const int32_t *qorder, int64_t m, int first, int chunk_rows, int nchunks,
                        uint32_t *keys, uint32_t *keys_out, int32_t *vals, int32_t *slots,
                        void *temp, size_t temp_bytes, cudaStream_t s);
 int launch_cluster_layout(const uint64_t *skeys, const int32_t *perm, int64_t n,
