@@ -53,33 +53,51 @@ namespace knnsweet {
 // Register budget: the dimension comes from the kernel parameters where it is
 // needed and `lostmin` lives in a shared-memory word of the warp, so neither
 // occupies a register through the scan loop.
+//
+// The warp's shared-memory slot holds, at fixed key offsets behind the
+// buffer, `lostmin` (the smallest FP32 d^2 dropped for lack of room, +inf:
+// none) and the current query's statistics words (kStat*), updated by lane
+// 0: kept out of registers, which the scan loop needs.
+enum { kStatPushed = 0, kStatMerges, kStatVisited, kStatPruned, kStatChecked, kStatWords = 6 };
+
+template <int kLostOff, int kStatOff>
 struct TopKBase {
   uint64_t *buf;  // append buffer (shared memory)
-  float *lostmin; // smallest FP32 d^2 dropped for lack of room (+inf: none)
   int nbuf, nlist, k;
-  uint64_t thr;   // a candidate enters iff its key < thr
+  // a candidate (d^2, index) enters iff d^2 <= thr_d2: the threshold key
+  // (thr_d2, 0xffffffff) lies above every key with that distance word
+  float thr_d2;
   float theta;    // distance matching thr (bound for the pruning tests)
-  unsigned pushed = 0, merges = 0;  // statistics of the current query (warp-uniform)
+
+  __device__ __forceinline__ float *lostmin() const {
+    return reinterpret_cast<float *>(buf + kLostOff);
+  }
+  __device__ __forceinline__ unsigned *stat() const {
+    return reinterpret_cast<unsigned *>(buf + kStatOff);
+  }
+  __device__ __forceinline__ void count(int which, unsigned v, int lane) const {
+    if (lane == 0) stat()[which] += v;
+  }
 
   __device__ __forceinline__ void reset_threshold(float th0, int lane) {
     nbuf = 0;
     nlist = 0;
     theta = th0;
-    if (lane == 0) *lostmin = __int_as_float(0x7f800000);
+    if (lane == 0) *lostmin() = __int_as_float(0x7f800000);
     // admits every d^2 <= th0^2, whatever the index
-    thr = ((uint64_t)__float_as_uint(th0 * th0) << 32) | 0xffffffffull;
+    thr_d2 = th0 * th0;
   }
   // threshold once the k-th squared distance is T: the FP32 band above it
   __device__ __forceinline__ void set_band_threshold(float T, int d) {
     const float W = band_hi(T, d);
-    thr = ((uint64_t)__float_as_uint(W) << 32) | 0xffffffffull;
+    thr_d2 = W;
     theta = sqrtf(W);
   }
   // a dropped key's distance word (NaN from an empty key is ignored)
   __device__ __forceinline__ void note_lost(uint32_t d2bits, int lane) {
     const float v = __uint_as_float(__reduce_min_sync(kFull, d2bits));
     __syncwarp();
-    if (lane == 0) *lostmin = fminf(*lostmin, v);
+    if (lane == 0) *lostmin() = fminf(*lostmin(), v);
     __syncwarp();
   }
 };
@@ -88,21 +106,21 @@ struct TopKBase {
 // (one key per lane), with the FP32 band of the k-th kept behind it as far as
 // the 32 slots allow.
 template <int E>
-struct RegTopK : TopKBase {
+struct RegTopK : TopKBase<64 * E + 2, 64 * E + 3> {
+  using B = TopKBase<64 * E + 2, 64 * E + 3>;
+  using B::buf, B::nbuf, B::nlist, B::k, B::count, B::note_lost, B::set_band_threshold,
+      B::reset_threshold;
   static constexpr int L = 32 * E;
   static constexpr int kCap = L;  // candidate buffer capacity
   // append buffer (L keys), L doubles for the FP64 band, 2 pivot words,
-  // lostmin
-  static constexpr int kSmemKeys = 2 * L + 3;
+  // lostmin, statistics
+  static constexpr int kSmemKeys = 2 * L + 3 + kStatWords / 2;
   static constexpr int kBandScratch = L, kPivot = 2 * L;
   uint64_t v[E];
 
   __device__ __forceinline__ int cap() const { return kCap; }
 
-  __device__ __forceinline__ void init(uint64_t *wsm) {
-    buf = wsm;
-    lostmin = reinterpret_cast<float *>(wsm + 2 * L + 2);
-  }
+  __device__ __forceinline__ void init(uint64_t *wsm) { buf = wsm; }
 
   __device__ __forceinline__ void reset(float th0, int lane) {
 #pragma unroll
@@ -137,7 +155,7 @@ struct RegTopK : TopKBase {
     note_lost(lost, lane);
     reg_bitonic_merge<E>(v, lane);
     nlist = min(k, nlist + nbuf);
-    merges++;
+    count(kStatMerges, 1, lane);
     nbuf = 0;
     if (nlist == k) {
       const int kl = (k - 1) / E, kj = (k - 1) % E;
@@ -205,14 +223,20 @@ __device__ __forceinline__ void smem_bitonic_sort(uint64_t *s, int lane) {
 #endif
 
 template <int LL>
-struct SelectTopK : TopKBase {
+struct SelectTopK : TopKBase<2 * LL + 128, 2 * LL + 129> {
+  using B = TopKBase<2 * LL + 128, 2 * LL + 129>;
+  using B::buf, B::nbuf, B::nlist, B::k, B::count, B::note_lost, B::set_band_threshold,
+      B::reset_threshold;
   static constexpr int L = LL;          // final sort length (pow2 >= k)
   static constexpr int kCap = 2 * LL;   // candidate capacity
-  static constexpr int kSmemKeys = 2 * LL + 129;  // keys, 256-word histogram, lostmin
+  // keys, 256-word histogram, lostmin, statistics
+  static constexpr int kSmemKeys = 2 * LL + 129 + kStatWords / 2;
   // after the final sort: LL doubles for the FP64 band behind the sorted
   // keys, the pivot in the histogram's words
   static constexpr int kBandScratch = LL, kPivot = 2 * LL;
-  uint32_t *hist;
+  __device__ __forceinline__ uint32_t *hist() const {
+    return reinterpret_cast<uint32_t *>(buf + 2 * LL);
+  }
 
   // A compaction once k + kEarly candidates are in (capacity permitting)
   // tightens the threshold sooner.  k = 200 self-join scan: capacity only
@@ -222,11 +246,7 @@ struct SelectTopK : TopKBase {
   static constexpr int kEarly = KNN_TOPK_EARLY;
   __device__ __forceinline__ int cap() const { return k + kEarly < kCap ? k + kEarly : kCap; }
 
-  __device__ __forceinline__ void init(uint64_t *wsm) {
-    buf = wsm;
-    hist = reinterpret_cast<uint32_t *>(wsm + 2 * LL);
-    lostmin = reinterpret_cast<float *>(wsm + 2 * LL + 128);
-  }
+  __device__ __forceinline__ void init(uint64_t *wsm) { buf = wsm; }
 
   __device__ __forceinline__ void reset(float th0, int lane) { reset_threshold(th0, lane); }
 
@@ -235,7 +255,7 @@ struct SelectTopK : TopKBase {
   __device__ __forceinline__ void flush(int lane, int d) {
     if (nbuf <= k) return;
     __syncwarp();
-    const uint64_t kth = warp_select_kth(buf, nbuf, k, hist, lane);
+    const uint64_t kth = warp_select_kth(buf, nbuf, k, hist(), lane);
     __syncwarp();
     int w = 0;
     uint32_t lost = 0xffffffffu;
@@ -253,7 +273,7 @@ struct SelectTopK : TopKBase {
     note_lost(lost, lane);
     nbuf = w;  // == k
     nlist = k;
-    merges++;
+    count(kStatMerges, 1, lane);
     set_band_threshold(key_d2(kth), d);
   }
 
@@ -269,10 +289,10 @@ struct SelectTopK : TopKBase {
 #if KNN_LINEAR_SELECT
     // an upper bound of the k-th: the threshold it gives admits a little more
     const uint32_t T = warp_kth_upper_u32(reinterpret_cast<const uint32_t *>(buf) + 1, 2,
-                                          nbuf, k, hist, lane);
+                                          nbuf, k, hist(), lane);
 #else
     const uint32_t T = warp_select_kth_u32(reinterpret_cast<const uint32_t *>(buf) + 1, 2,
-                                           nbuf, k, hist, lane);
+                                           nbuf, k, hist(), lane);
 #endif
     const uint32_t W = __float_as_uint(band_hi(__uint_as_float(T), d));
     int w = 0;
@@ -291,7 +311,7 @@ struct SelectTopK : TopKBase {
       flush(lane, d);
       return;
     }
-    merges++;
+    count(kStatMerges, 1, lane);
     nlist = k;
     set_band_threshold(__uint_as_float(T), d);
   }
@@ -327,7 +347,7 @@ struct SelectTopK : TopKBase {
       // bitonic network alone); the network where equal distances crowd a bin
 #if KNN_BIN_SORT
       if constexpr (LL <= 256)  // the bin tags of 8 keys per lane stay in registers
-        if (warp_bin_sort<LL / 32>(buf, nbuf, buf + LL, hist, lane)) return nbuf;
+        if (warp_bin_sort<LL / 32>(buf, nbuf, buf + LL, hist(), lane)) return nbuf;
 #endif
       for (int i = nbuf + lane; i < LL; i += 32) buf[i] = kKeyMax;
       __syncwarp();
@@ -349,13 +369,13 @@ __device__ __forceinline__ void topk_offer(TK &tk, bool pass, float v, int32_t i
   int cnt = __popc(b);
   if (tk.nbuf + cnt > tk.cap()) {
     tk.make_room(lane, d);
-    pass = pass && v <= key_d2(tk.thr);
+    pass = pass && v <= tk.thr_d2;
     b = __ballot_sync(kFull, pass);
     cnt = __popc(b);
   }
   if (pass) tk.buf[tk.nbuf + __popc(b & ((1u << lane) - 1))] = make_key(v, idx);
   tk.nbuf += cnt;
-  tk.pushed += cnt;
+  tk.count(kStatPushed, cnt, lane);
 }
 
 // Whether every FP32 squared distance of the join is exact (both sides hold
@@ -460,7 +480,7 @@ __device__ __forceinline__ unsigned emit_query(TK &tk, const ScanArgs &a, int32_
       nlo += __popc(__ballot_sync(kFull, v < lo));
       nhi += __popc(__ballot_sync(kFull, v <= hi));
     }
-    if (*tk.lostmin <= hi) {
+    if (*tk.lostmin() <= hi) {
       defer = true;
     } else if (nhi > k) {
       band_resolve_fp64(s, nlo, nhi, k, a.d, a.dp4,
@@ -608,13 +628,14 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
   tk.init(keys_base + (size_t)w * TK::kSmemKeys);
   tk.k = a.k;
   const float tol = bound_tol(a.d);
-  unsigned evals = 0, visited = 0, pruned = 0, checked = 0;
+  unsigned evals = 0;
   // small rows: load the member row together with its band distance
   constexpr bool kEagerRow = KNN_EAGER_ROWS && (DP4 > 0 && DP4 <= 2);
   // statistics: per-lane 32-bit counts folded once per query into per-block
   // shared counters, added to the global ones at exit
   __shared__ unsigned long long blk_ctr[kScanCounters];
   if (threadIdx.x < kScanCounters) blk_ctr[threadIdx.x] = 0;
+  if (lane < kStatWords) tk.stat()[lane] = 0;
   __syncthreads();
 
   for (;;) {
@@ -675,7 +696,7 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
       bool pass = false;
       if (inb) {
         evals++;
-        pass = v <= key_d2(tk.thr);
+        pass = v <= tk.thr_d2;
         if (!IDXROW && pass) idx = a.sidx[gp];
       }
       topk_offer(tk, pass, v, idx, lane, a.d);
@@ -709,11 +730,11 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
 #else
         alive = !(D - a.cmax[rs] > th + slack) && !(D + th + slack < a.cmin[rs]);
 #endif
-        if (!alive) pruned++;
       }
       // visit this chunk's surviving clusters: in list order (by rep-rep
       // distance) or, with KNN_ORDER_BY_D, nearest d(q, Rs) first
       unsigned amask = __ballot_sync(kFull, alive);
+      tk.count(kStatPruned, (unsigned)(min(32, nr - base) - __popc(amask)), lane);
       if (amask == 0) continue;  // warp-uniform: nothing to visit in this batch
       const int nalive = __popc(amask);
       float dkey = alive ? D : __int_as_float(0x7f800000);
@@ -776,10 +797,10 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
         float th = tk.theta;
         float slack = tol * (2.0f * Dc + 2.0f * th);
         if (Dc - cmax_c > th + slack || Dc + th + slack < cmin_c) {
-          if (lane == 0) pruned++;
+          tk.count(kStatPruned, 1, lane);
           continue;
         }
-        if (lane == 0) visited++;
+        tk.count(kStatVisited, 1, lane);
 #if KNN_VISIT_META
         const int start = __shfl_sync(kFull, cst, src);
         const int n_c = __shfl_sync(kFull, cnn, src);
@@ -840,25 +861,24 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
       }
     }
     tk.finish(lane, a.d);
-    checked += emit_query(tk, a, (int32_t)slot, q, qc, lane);
+    tk.count(kStatChecked, emit_query(tk, a, (int32_t)slot, q, qc, lane), lane);
+    __syncwarp();
     if (a.counters) {
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        evals += __shfl_xor_sync(kFull, evals, o);
-        visited += __shfl_xor_sync(kFull, visited, o);
-        pruned += __shfl_xor_sync(kFull, pruned, o);
-      }
+      for (int o = 16; o > 0; o >>= 1) evals += __shfl_xor_sync(kFull, evals, o);
       if (lane == 0) {
+        const unsigned *st = tk.stat();
         atomicAdd(&blk_ctr[0], (unsigned long long)evals);
-        atomicAdd(&blk_ctr[1], (unsigned long long)visited);
-        atomicAdd(&blk_ctr[2], (unsigned long long)pruned);
-        atomicAdd(&blk_ctr[3], (unsigned long long)tk.pushed);
-        atomicAdd(&blk_ctr[4], (unsigned long long)tk.merges);
-        atomicAdd(&blk_ctr[5], (unsigned long long)checked);
+        atomicAdd(&blk_ctr[1], (unsigned long long)st[kStatVisited]);
+        atomicAdd(&blk_ctr[2], (unsigned long long)st[kStatPruned]);
+        atomicAdd(&blk_ctr[3], (unsigned long long)st[kStatPushed]);
+        atomicAdd(&blk_ctr[4], (unsigned long long)st[kStatMerges]);
+        atomicAdd(&blk_ctr[5], (unsigned long long)st[kStatChecked]);
       }
     }
-    evals = visited = pruned = checked = 0;
-    tk.pushed = tk.merges = 0;
+    __syncwarp();
+    if (lane < kStatWords) tk.stat()[lane] = 0;
+    evals = 0;
   }
   __syncthreads();
   if (a.counters && threadIdx.x < kScanCounters)
