@@ -24,7 +24,9 @@
  *  - Every call returns 0 (KNN_OK) or a negative KNN_E* code and never exits
  *    the process; knn_last_error() gives a message (per host thread).
  *  - Calls hold no global state and may run concurrently from several host
- *    threads; each call uses one CUDA stream.
+ *    threads; each device-buffer call uses the caller's stream, each
+ *    host-buffer call two streams of the calling thread (created on its first
+ *    host-buffer call on a device and reused; idle between calls).
  */
 #ifndef KNNSWEET_H
 #define KNNSWEET_H
@@ -230,7 +232,7 @@ int knn_join_batched_device(const float *q, const int64_t *q_offsets,
  * knn_join_batched_device on HOST buffers: q, r, out_idx and out_dist are host
  * memory (the reference keeps its inputs and result in host arrays,
  * src/knnjoin.cu:1003-1033, and runs one pair of point sets per process).  The
- * clouds are copied to the current device on a stream of the call's own,
+ * clouds are copied to the current device on a stream of the calling thread,
  * joined, and the result copied back; the call returns when it is complete.
  * Offsets, limits, options and results as for knn_join_batched_device.
  */

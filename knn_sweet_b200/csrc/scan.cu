@@ -56,9 +56,13 @@ namespace knnsweet {
 //
 // The warp's shared-memory slot holds, at fixed key offsets behind the
 // buffer, `lostmin` (the smallest FP32 d^2 dropped for lack of room, +inf:
-// none) and the current query's statistics words (kStat*), updated by lane
-// 0: kept out of registers, which the scan loop needs.
-enum { kStatPushed = 0, kStatMerges, kStatVisited, kStatPruned, kStatChecked, kStatWords = 6 };
+// none), the current query's statistics words (kStat*, updated by lane 0)
+// and the query's slot, row and cluster (kSide*, needed only when the query
+// starts and ends): kept out of registers, which the scan loop needs.
+enum {
+  kStatPushed = 0, kStatMerges, kStatVisited, kStatPruned, kStatChecked,
+  kSideSlot, kSideQuery, kSideCluster, kStatWords
+};
 
 template <int kLostOff, int kStatOff>
 struct TopKBase {
@@ -597,6 +601,17 @@ struct QueryRow<0, IDXROW> {
 #define KNN_INDEX32 1
 #endif
 
+// The thread-per-query scan keeps its statistics counters in shared memory
+// (1) or in registers (0).
+#ifndef KNN_TSCAN_SMEM_STATS
+#define KNN_TSCAN_SMEM_STATS 1
+#endif
+// The query's slot, row and cluster wait out the walk in shared memory (1)
+// or in registers (0).
+#ifndef KNN_SIDE_WORDS
+#define KNN_SIDE_WORDS 1
+#endif
+
 // Largest k kept in a register list (one key per lane): up to 24, so that
 // 8 of the 32 slots or more hold the FP32 band behind the k-th; larger k use
 // the shared-memory candidate set.
@@ -652,6 +667,14 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
     }
     const int64_t q = a.qorder[slot];
     const int qc = a.slot_cl[slot];
+#if KNN_SIDE_WORDS
+    if (lane == 0) {
+      unsigned *sw = tk.stat();
+      sw[kSideSlot] = (unsigned)slot;
+      sw[kSideQuery] = (unsigned)q;
+      sw[kSideCluster] = (unsigned)qc;
+    }
+#endif
     QueryRow<DP4, IDXROW> qr;
     qr.load(a.qrows, q, dp4, qslot);
     tk.reset(query_theta0(a, slot, qc, tol), lane);
@@ -861,7 +884,18 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
       }
     }
     tk.finish(lane, a.d);
+#if KNN_SIDE_WORDS
+    __syncwarp();
+    {
+      const unsigned *sw = tk.stat();
+      const int32_t e_slot = (int32_t)sw[kSideSlot];
+      const int64_t e_q = (int64_t)sw[kSideQuery];
+      const int e_qc = (int)sw[kSideCluster];
+      tk.count(kStatChecked, emit_query(tk, a, e_slot, e_q, e_qc, lane), lane);
+    }
+#else
     tk.count(kStatChecked, emit_query(tk, a, (int32_t)slot, q, qc, lane), lane);
+#endif
     __syncwarp();
     if (a.counters) {
 #pragma unroll
@@ -965,7 +999,16 @@ __global__ void __launch_bounds__(256, 4)
   __syncthreads();
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t nslots = a.slot_list ? (int64_t)*a.slot_count : a.m;
+#if KNN_TSCAN_SMEM_STATS
+  // visited, pruned, pushed of this thread's query in shared memory (stride
+  // 3 words: no bank conflicts), out of the walk's registers
+  __shared__ unsigned tstat[3 * 256];
+  unsigned *ts = tstat + 3 * threadIdx.x;
+  ts[0] = ts[1] = ts[2] = 0;
+  unsigned evals = 0;
+#else
   unsigned evals = 0, visited = 0, pruned = 0, pushed = 0;
+#endif
   if (t < nslots) {
     const int64_t slot = a.slot_list ? (int64_t)a.slot_list[t] : a.slot_base + t;
     const int64_t q = a.qorder[slot];
@@ -988,10 +1031,18 @@ __global__ void __launch_bounds__(256, 4)
       float slack = tol * (2.0f * D + 2.0f * theta);
       const float cmin = a.cmin[c];
       if (D - a.cmax[c] > theta + slack || D + theta + slack < cmin) {
+#if KNN_TSCAN_SMEM_STATS
+        ts[1]++;
+#else
         pruned++;
+#endif
         continue;
       }
+#if KNN_TSCAN_SMEM_STATS
+      ts[0]++;
+#else
       visited++;
+#endif
       const int start = a.soff[c], n_c = a.soff[c + 1] - start;
       const float *sd = a.sdist + start;
       // first member of the band [D - theta, D + theta] (with slack)
@@ -1019,7 +1070,11 @@ __global__ void __launch_bounds__(256, 4)
           if (key < tk.key[K - 1]) {
             lost = fminf(lost, key_d2(tk.key[K - 1]));  // NaN (empty) is ignored
             tk.insert(key);
+#if KNN_TSCAN_SMEM_STATS
+            ts[2]++;
+#else
             pushed++;
+#endif
             if (tk.key[K - 1] != kKeyMax) {
               theta = sqrtf(band_hi(key_d2(tk.key[K - 1]), d));
               slack = tol * (2.0f * D + 2.0f * theta);
@@ -1075,6 +1130,9 @@ __global__ void __launch_bounds__(256, 4)
     }
   }
   if (a.counters) {
+#if KNN_TSCAN_SMEM_STATS
+    unsigned visited = ts[0], pruned = ts[1], pushed = ts[2];
+#endif
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       evals += __shfl_xor_sync(kFull, evals, o);
