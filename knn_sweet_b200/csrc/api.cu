@@ -419,8 +419,9 @@ int build_query_side(const RefSide &R, bool share, const float *q, int64_t m, in
   KNN_TRY(ar.alloc(&Q->theta0, (size_t)Rq));
   KNN_TRY(ar.alloc(&Q->rlist, (size_t)Rq * Rs));
   KNN_TRY(ar.alloc(&Q->rlen, (size_t)Rq));
+  KNN_TRY(ar.alloc(&Q->clb, (size_t)Rq * ((Rs + 31) / 32)));
   KNN_TRY(launch_bounds_filter(Q->drr, Rq, Rs, Q->qrad, Q->qset.off, R.sset.off, R.sdist, R.cmax,
-                               k, d, Q->theta0, Q->rlist, Q->rlen, s));
+                               k, d, Q->theta0, Q->rlist, Q->rlen, Q->clb, s));
   return KNN_OK;
 }
 
@@ -482,6 +483,9 @@ int search_clusters(const RefSide &R, const QuerySide &Q, int64_t m, int32_t k, 
     t.rlist = Q.rlist;
     t.rlen = Q.rlen;
     t.Rs = Rs;
+    t.clb = Q.clb;
+    t.clb_stride = (Rs + 31) / 32;
+    t.qkeys = Q.qset.skeys;
     t.theta0 = Q.theta0;
     t.k = k;
     t.cap = cap;
@@ -523,6 +527,8 @@ int search_clusters(const RefSide &R, const QuerySide &Q, int64_t m, int32_t k, 
   a.qkeys = Q.qset.skeys;
   a.rlist = Q.rlist;
   a.rlen = Q.rlen;
+  a.clb = Q.clb;
+  a.clb_stride = (Rs + 31) / 32;
   a.Rs = Rs;
   a.n_ref = R.n;
   a.rrows = R.Rp;

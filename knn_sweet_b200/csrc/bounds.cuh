@@ -35,7 +35,7 @@ static __device__ __forceinline__ void bounds_filter_block(const float *dq, int 
                                     const float *__restrict__ scmax, float rq, int k, int d,
                                     int rs_pow2, int32_t id_base, uint64_t *skey,
                                     float *theta0_out, int32_t *rlist_out,
-                                    int32_t *rlen_out) {
+                                    int32_t *rlen_out, float2 *chunk_out = nullptr) {
   __shared__ int red_i[32];
   __shared__ unsigned red_u[32], red_l[32];
   __shared__ int kept_s;
@@ -162,6 +162,31 @@ static __device__ __forceinline__ void bounds_filter_block(const float *dq, int 
   for (int j = tid; j < kept; j += nth)
     rlist_out[j] = id_base + (int32_t)(skey[j] & 0xffffffffu);
   if (tid == 0) *rlen_out = kept;
+  if (chunk_out && warp == 0) {
+    // per chunk of 32 list entries: the first entry's d(Rq, Rs) (the list
+    // is ascending in it) and the largest radius from that entry to the end,
+    // by suffix maxima over the chunks, 32 chunks per round from the back
+    const int nch = (kept + 31) >> 5;
+    float carry = 0.0f;
+    for (int c0 = (nch - 1) & ~31; c0 >= 0; c0 -= 32) {
+      const int c = c0 + lane;
+      float m = 0.0f, first = 0.0f;
+      if (c < nch) {
+        const int e1 = min(32 * c + 32, kept);
+        for (int e = 32 * c; e < e1; e++)
+          m = fmaxf(m, scmax[(int32_t)(skey[e] & 0xffffffffu)]);
+        first = __uint_as_float((uint32_t)(skey[32 * c] >> 32));
+      }
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const float t = __shfl_down_sync(kFull, m, o);
+        if (lane + o < 32) m = fmaxf(m, t);
+      }
+      m = fmaxf(m, carry);
+      carry = __shfl_sync(kFull, m, 0);
+      if (c < nch) chunk_out[c] = make_float2(first, m);
+    }
+  }
 }
 
 // The same bound and candidate list by one warp, for query clusters with few

@@ -527,7 +527,7 @@ __global__ void __launch_bounds__(512)
                          const float *__restrict__ scmax, int k, int d,
                          int rs_pow2, float *__restrict__ theta0,
                          int32_t *__restrict__ rlist,
-                         int32_t *__restrict__ rlen) {
+                         int32_t *__restrict__ rlen, float2 *__restrict__ clb) {
   extern __shared__ uint64_t skey[];
   const int qc = blockIdx.x;
   if (qoff[qc + 1] == qoff[qc]) {  // empty query cluster
@@ -538,7 +538,8 @@ __global__ void __launch_bounds__(512)
     return;
   }
   bounds_filter_block(drr + (int64_t)qc * Rs, Rs, soff, sdist, scmax, qrad[qc], k, d, rs_pow2,
-                      0, skey, theta0 + qc, rlist + (int64_t)qc * Rs, rlen + qc);
+                      0, skey, theta0 + qc, rlist + (int64_t)qc * Rs, rlen + qc,
+                      clb ? clb + (int64_t)qc * ((Rs + 31) / 32) : nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -812,7 +813,7 @@ int launch_bounds_filter(const float *drr, int Rq, int Rs, const float *qrad,
                          const int32_t *qoff, const int32_t *soff,
                          const float *sdist, const float *scmax, int k, int d,
                          float *theta0, int32_t *rlist, int32_t *rlen,
-                         cudaStream_t s) {
+                         float2 *clb, cudaStream_t s) {
   int p2 = 1;
   while (p2 < Rs) p2 <<= 1;
   size_t smem = (size_t)p2 * sizeof(uint64_t);
@@ -821,7 +822,7 @@ int launch_bounds_filter(const float *drr, int Rq, int Rs, const float *qrad,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
   bounds_filter_kernel<<<Rq, 512, smem, s>>>(drr, Rq, Rs, qrad, qoff, soff, sdist,
-                                             scmax, k, d, p2, theta0, rlist, rlen);
+                                             scmax, k, d, p2, theta0, rlist, rlen, clb);
   KNN_LAUNCH_CHECK();
   return KNN_OK;
 }

@@ -4,6 +4,12 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// A query (a tile of queries) stops walking its candidate list where the
+// rest of it is prunable as a whole (1), or tests every entry (0).
+#ifndef KNN_CHUNK_EXIT
+#define KNN_CHUNK_EXIT 1
+#endif
+
 namespace knnsweet {
 
 // Statistics the scan kernels accumulate (ScanArgs::counters): distance
@@ -33,6 +39,10 @@ struct ScanArgs {
                             // query's own bound theta0 - (rq - d(q,Rq)); null: theta0
   const int32_t *rlist;     // Rq x Rs surviving clusters, nearest first
   const int32_t *rlen;      // Rq
+  const float2 *clb;        // optional (null: none): per query cluster and 32
+                            // list entries, x = d(Rq, Rs) of the chunk's first
+                            // entry, y = the largest radius from that entry on
+  int clb_stride;           // chunks per query cluster in clb
   const int64_t *rl_base;   // batched form: start of each query cluster's list
                             // in rlist (null: qc * Rs)
   const int64_t *qc_ref_base;  // batched form: subtracted from every output
@@ -106,7 +116,7 @@ int launch_bounds_filter(const float *drr, int Rq, int Rs, const float *qrad,
                          const int32_t *qoff, const int32_t *soff,
                          const float *sdist, const float *scmax, int k, int d,
                          float *theta0, int32_t *rlist, int32_t *rlen,
-                         cudaStream_t s);
+                         float2 *clb, cudaStream_t s);
 int launch_scan(const ScanArgs &a, int num_sms, cudaStream_t s);
 
 // Arguments of the BF16 tensor-core tile search with FP32 re-ranking
@@ -128,6 +138,9 @@ struct TileArgs {
   const int32_t *rlist;      // Rq x Rs surviving clusters, nearest first
   const int32_t *rlen;       // Rq
   int Rs;
+  const float2 *clb;         // optional: per list chunk, as ScanArgs::clb
+  int clb_stride;
+  const uint64_t *qkeys;     // slot -> (cluster, d(q, Rq)) key (with clb)
   const float *theta0;       // Rq: k-th distance bound per query cluster
   int k, cap, P;             // k; buffer entries per query; sort scratch (pow2)
   bool squared;

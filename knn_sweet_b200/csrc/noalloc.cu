@@ -323,7 +323,7 @@ int noalloc_join(const float *q, int64_t m, const float *r, int64_t n, int32_t d
   if (rc == KNN_OK) rc = launch_rep_dist(Qb.reps, p.Rq, p.S.reps, p.Rs, p.dp4s, p.drr, s);
   if (rc == KNN_OK)
     rc = launch_bounds_filter(p.drr, p.Rq, p.Rs, p.qrad, Qb.off, p.S.off, p.sdist, p.cmax,
-                              k, d, p.theta0, p.rlist, p.rlen, s);
+                              k, d, p.theta0, p.rlist, p.rlen, nullptr, s);
   if (rc != KNN_OK) return rc;
   ScanArgs a{};
   a.qrows = Qp;

@@ -123,6 +123,7 @@ struct QuerySide {
   const int *inexact = nullptr;
   float *qrad = nullptr, *drr = nullptr, *theta0 = nullptr;
   int32_t *slot_cl = nullptr, *rlist = nullptr, *rlen = nullptr;
+  float2 *clb = nullptr;  // per list chunk: first d(Rq, Rs), largest radius from it on
 };
 
 // Argument and option ranges shared by every entry point.

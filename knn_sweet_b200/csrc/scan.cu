@@ -61,8 +61,9 @@ namespace knnsweet {
 // starts and ends): kept out of registers, which the scan loop needs.
 enum {
   kStatPushed = 0, kStatMerges, kStatVisited, kStatPruned, kStatChecked,
-  kSideSlot, kSideQuery, kSideCluster, kStatWords
+  kSideSlot, kSideQuery, kSideCluster, kSideDq, kStatWords
 };
+constexpr int kStatKeys = (kStatWords + 1) / 2;  // 64-bit words they take
 
 template <int kLostOff, int kStatOff>
 struct TopKBase {
@@ -118,7 +119,7 @@ struct RegTopK : TopKBase<64 * E + 2, 64 * E + 3> {
   static constexpr int kCap = L;  // candidate buffer capacity
   // append buffer (L keys), L doubles for the FP64 band, 2 pivot words,
   // lostmin, statistics
-  static constexpr int kSmemKeys = 2 * L + 3 + kStatWords / 2;
+  static constexpr int kSmemKeys = 2 * L + 3 + kStatKeys;
   static constexpr int kBandScratch = L, kPivot = 2 * L;
   uint64_t v[E];
 
@@ -234,7 +235,7 @@ struct SelectTopK : TopKBase<2 * LL + 128, 2 * LL + 129> {
   static constexpr int L = LL;          // final sort length (pow2 >= k)
   static constexpr int kCap = 2 * LL;   // candidate capacity
   // keys, 256-word histogram, lostmin, statistics
-  static constexpr int kSmemKeys = 2 * LL + 129 + kStatWords / 2;
+  static constexpr int kSmemKeys = 2 * LL + 129 + kStatKeys;
   // after the final sort: LL doubles for the FP64 band behind the sorted
   // keys, the pivot in the histogram's words
   static constexpr int kBandScratch = LL, kPivot = 2 * LL;
@@ -644,6 +645,7 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
   tk.k = a.k;
   const float tol = bound_tol(a.d);
   unsigned evals = 0;
+  constexpr bool kWideRows = DP4 == 0 || DP4 >= 4;
   // small rows: load the member row together with its band distance
   constexpr bool kEagerRow = KNN_EAGER_ROWS && (DP4 > 0 && DP4 <= 2);
   // statistics: per-lane 32-bit counts folded once per query into per-block
@@ -673,6 +675,7 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
       sw[kSideSlot] = (unsigned)slot;
       sw[kSideQuery] = (unsigned)q;
       sw[kSideCluster] = (unsigned)qc;
+      sw[kSideDq] = a.qkeys ? (uint32_t)a.qkeys[slot] : 0x7f800000u;  // +inf: no exit
     }
 #endif
     QueryRow<DP4, IDXROW> qr;
@@ -729,6 +732,24 @@ __global__ void __launch_bounds__(WARPS * 32, (scan_min_blocks<DP4, WARPS>()))
     const int nr = a.rlen[qc];
     const int32_t *rl = a.rlist + (a.rl_base ? a.rl_base[qc] : (int64_t)qc * a.Rs);
     for (int base = 0; base < nr; base += 32) {
+#if KNN_CHUNK_EXIT && KNN_SIDE_WORDS
+      // the rest of the list is prunable when even its nearest cluster
+      // (the list is ascending in d(Rq,Rs)) lies beyond theta for the
+      // largest remaining radius: d(q,Rs) - cmax >= d(Rq,Rs) - d(q,Rq) -
+      // max cmax; the filter's own test, with twice its rounding margin.
+      // Rows of 16 floats or more (d = 32: scan 6.14 -> 5.61 ms, d = 128:
+      // 14.88 -> 13.42 ms); on the k = 200, d = 3 self-join the test cost
+      // more than it saved (3.82 -> 3.87 ms)
+      if (kWideRows && a.clb) {
+        const unsigned *sw = tk.stat();
+        const float2 cb = a.clb[(size_t)sw[kSideCluster] * a.clb_stride + (base >> 5)];
+        const float dqv = __uint_as_float(sw[kSideDq]), th = tk.theta;
+        if (cb.x - dqv - cb.y > th + 2.0f * tol * (cb.x + dqv + cb.y + th)) {
+          tk.count(kStatPruned, (unsigned)(nr - base), lane);
+          break;
+        }
+      }
+#endif
       const int j = base + lane;
       int rs = 0;
       float D = 0.0f;

@@ -139,6 +139,8 @@ int replicate_sides(Arena &ar, int g, int g0, const RefSide &R, const QuerySide 
   KNN_TRY(replicate(ar, g, g0, Q.qset.skeys, (size_t)m, s, &Q2->qset.skeys));
   KNN_TRY(replicate(ar, g, g0, Q.rlist, (size_t)Rq * Rs, s, &Q2->rlist));
   KNN_TRY(replicate(ar, g, g0, Q.rlen, (size_t)Rq, s, &Q2->rlen));
+  if (Q.clb)
+    KNN_TRY(replicate(ar, g, g0, Q.clb, (size_t)Rq * ((Rs + 31) / 32), s, &Q2->clb));
   return KNN_OK;
 }
 

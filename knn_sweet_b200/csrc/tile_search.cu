@@ -392,6 +392,10 @@ __global__ void __launch_bounds__(NT, NT == kTM ? 4 : 2)
     const float qb = row_thread ? 2.02f * (sqrtf(s_e[tid]) + gtc * sqrtf(s_t[tid])) : 0.0f;
     const float th = a.theta0[qc];
     float tau = th * th * 1.0009765625f;
+    // the row's distance to its representative, for the list's early exit
+    const float dq_row = valid && a.clb && a.qkeys
+                             ? __uint_as_float((uint32_t)a.qkeys[s0 + tid])
+                             : __int_as_float(0x7f800000);
     int n = 0;
     bool ovf = false;
     __syncthreads();  // the row sums are reused for the member rows below
@@ -448,6 +452,20 @@ __global__ void __launch_bounds__(NT, NT == kTM ? 4 : 2)
     // the first batch holds the four nearest clusters only: they tighten the
     // bounds before the rest of the list is decided
     for (int jb = 0, nb = 0; jb < nl && ok; jb += nb) {
+#if KNN_CHUNK_EXIT
+      // the rest of the list is prunable for every query of the tile: its
+      // nearest cluster's d(Rq, Rs) (the chunk of jb starts at or before
+      // it), less the row's d(q, Rq) and the largest radius from there on,
+      // beyond the row's bound (the filter's test, twice its margin)
+      if (a.clb && jb > 0) {
+        bool done = true;
+        if (valid) {
+          const float2 cb = a.clb[(size_t)qc * a.clb_stride + (jb >> 5)];
+          done = cb.x - dq_row - cb.y > th_q + 2.0f * tol * (cb.x + dq_row + cb.y + th_q);
+        }
+        if (__syncthreads_and(done)) break;
+      }
+#endif
       nb = jb == 0 ? min(4, nl) : min(kTN, nl - jb);
       stage_tile<NT>(
           sb, sc, KD, d, dp4,
