@@ -103,6 +103,16 @@ __global__ void reps_to_bf16_tiles_kernel(const float4 *__restrict__ reps, int R
 // epilogue warps split the TN columns kEsplit ways (4 measured no faster)
 constexpr int kEsplit = 2;
 constexpr int kAssignThreads = 128 * kEsplit + 32;
+// Representative tile width (MMA N) and the number of shared-memory tile
+// buffers the producer keeps in flight: a buffer is refilled with tile
+// j + kStages once MMA j has read it.
+#ifndef KNN_ASSIGN_TN
+#define KNN_ASSIGN_TN 128
+#endif
+#ifndef KNN_ASSIGN_STAGES
+#define KNN_ASSIGN_STAGES 2
+#endif
+constexpr int kStages = KNN_ASSIGN_STAGES;
 
 __global__ void __launch_bounds__(kAssignThreads, 1)
     assign_tc_kernel(const float4 *__restrict__ rows, int64_t n, int dp4, int d, int KD, int TN,
@@ -112,10 +122,10 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
   extern __shared__ __align__(1024) unsigned char smem[];
   const size_t a_bytes = tc::tile_bytes(kTileM, KD), b_bytes = tc::tile_bytes(TN, KD);
   unsigned char *sa = smem;
-  unsigned char *sb0 = sa + a_bytes, *sb1 = sb0 + b_bytes;
-  auto sb = [&](int b) { return b ? sb1 : sb0; };
-  uint64_t *full = reinterpret_cast<uint64_t *>(sb1 + b_bytes);
-  uint64_t *done = full + 2;
+  unsigned char *sb0 = sa + a_bytes;
+  auto sb = [&](int b) { return sb0 + (size_t)b * b_bytes; };
+  uint64_t *full = reinterpret_cast<uint64_t *>(sb0 + (size_t)kStages * b_bytes);
+  uint64_t *done = full + kStages;
   uint64_t *empty = done + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(empty + 2);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
@@ -129,8 +139,8 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
 
   if (warp == 0) tc::tmem_alloc(tmem_slot, ncols);
   if (tid == 0) {
+    for (int i = 0; i < kStages; i++) tc::mbar_init(full + i, 1);
     for (int i = 0; i < 2; i++) {
-      tc::mbar_init(full + i, 1);
       tc::mbar_init(done + i, 1);
       tc::mbar_init(empty + i, 4 * kEsplit);
     }
@@ -139,9 +149,10 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
   }
   __syncthreads();
   const bool producer = warp == 4 * kEsplit && lane == 0;
-  // first two representative tiles in flight while the points are staged
+  // the first kStages representative tiles in flight while the points are
+  // staged
   if (producer)
-    for (int j = 0; j < 2 && j < ntiles; j++) {
+    for (int j = 0; j < kStages && j < ntiles; j++) {
       tc::mbar_arrive_expect_tx(full + j, (uint32_t)b_bytes);
       tc::bulk_copy_g2s(sb(j), tiles_g + (size_t)j * b_bytes, (uint32_t)b_bytes, full + j);
     }
@@ -178,15 +189,15 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
       const uint32_t idesc = tc::make_idesc_bf16(kTileM, TN);
       const uint32_t a_base = tc::smem_u32(sa);
       const uint32_t sbo = (uint32_t)KD * 16;
-      int copies = ntiles < 2 ? ntiles : 2, mmas = 0;
-      // MMA of tile j into accumulator j & 1, once its copy landed and the
-      // epilogue released the accumulator (tile j - 2)
+      int copies = ntiles < kStages ? ntiles : kStages, mmas = 0;
+      // MMA of tile j (buffer j % kStages) into accumulator j & 1, once its
+      // copy landed and the epilogue released the accumulator (tile j - 2)
       auto issue = [&](int j) -> bool {
-        const int b = j & 1;
+        const int b = j & 1, bb = j % kStages;
         if (j >= 2 && !tc::mbar_wait(empty + b, (uint32_t)(((j - 2) >> 1) & 1))) return false;
-        if (!tc::mbar_wait(full + b, (uint32_t)((j >> 1) & 1))) return false;
+        if (!tc::mbar_wait(full + bb, (uint32_t)((j / kStages) & 1))) return false;
         tc::fence_after_sync();
-        const uint32_t b_base = tc::smem_u32(sb(b));
+        const uint32_t b_base = tc::smem_u32(sb(bb));
         for (int st = 0; st < KD / 16; st++) {
           const uint64_t ad = tc::make_desc(a_base + 256u * st, 128u, sbo);
           const uint64_t bd = tc::make_desc(b_base + 256u * st, 128u, sbo);
@@ -199,23 +210,24 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
       bool ok = ntiles == 0 || issue(0);
       for (int j = 0; ok && j < ntiles; j++) {
         if (*abort_flag) { ok = false; break; }
-        // queue MMA j + 1 behind MMA j, then refill buffer j & 1 with tile
-        // j + 2 once MMA j has read it
+        // queue MMA j + 1 behind MMA j, then refill MMA j's buffer with
+        // tile j + kStages once MMA j has read it
         if (j + 1 < ntiles && !issue(j + 1)) { ok = false; break; }
-        if (j + 2 < ntiles) {
-          const int b = j & 1;
-          if (!tc::mbar_wait(done + b, (uint32_t)((j >> 1) & 1))) { ok = false; break; }
-          tc::mbar_arrive_expect_tx(full + b, (uint32_t)b_bytes);
-          tc::bulk_copy_g2s(sb(b), tiles_g + (size_t)(j + 2) * b_bytes, (uint32_t)b_bytes,
-                            full + b);
-          copies = j + 3;
+        if (j + kStages < ntiles) {
+          const int bb = j % kStages;
+          if (!tc::mbar_wait(done + (j & 1), (uint32_t)((j >> 1) & 1))) { ok = false; break; }
+          tc::mbar_arrive_expect_tx(full + bb, (uint32_t)b_bytes);
+          tc::bulk_copy_g2s(sb(bb), tiles_g + (size_t)(j + kStages) * b_bytes,
+                            (uint32_t)b_bytes, full + bb);
+          copies = j + kStages + 1;
         }
       }
       if (!ok) {
         *abort_flag = 1;
         // let the copies and MMAs already issued finish before the CTA's
         // shared memory and TMEM go away (bounded waits)
-        for (int j = mmas; j < copies; j++) tc::mbar_wait(full + (j & 1), (uint32_t)((j >> 1) & 1));
+        for (int j = mmas; j < copies; j++)
+          tc::mbar_wait(full + j % kStages, (uint32_t)((j / kStages) & 1));
         if (mmas > 0) tc::mbar_wait(done + ((mmas - 1) & 1), (uint32_t)(((mmas - 1) >> 1) & 1));
       }
     }
@@ -317,9 +329,9 @@ int launch_assign_tc(const float4 *rows, int64_t n, int dp4, int d, const float4
   // representative tiles of 128 rows: a CTA then holds 256 TMEM columns and
   // two CTAs share an SM (measured faster than 256-row tiles with one CTA
   // per SM, with either 8 or 16 epilogue warps)
-  const int TN = kTileN / 2;
-  const size_t need = tc::tile_bytes(kTileM, KD) + 2 * tc::tile_bytes(TN, KD) +
-                      6 * sizeof(uint64_t) + 16 + (size_t)kEsplit * kTileM * 8;
+  const int TN = KNN_ASSIGN_TN;
+  const size_t need = tc::tile_bytes(kTileM, KD) + (size_t)kStages * tc::tile_bytes(TN, KD) +
+                      (kStages + 4) * sizeof(uint64_t) + 16 + (size_t)kEsplit * kTileM * 8;
   // a CTA holds 2 x TN TMEM columns: with TN = 256 that is all 512, so at
   // most one CTA per SM (over 114 KB each), with TN = 128 at most two
   const size_t smem = std::max<size_t>(need, TN == kTileN ? 116 * 1024 : 80 * 1024);
