@@ -76,12 +76,15 @@ def knn_chamfer(x: torch.Tensor, y: torch.Tensor, k: int = 1) -> torch.Tensor:
 
 
 def _cloud_base(offsets, rows_off, device):
-    """Per query row: the first row of its cloud's reference points."""
+    """Per query row: the first row of its cloud's reference points.  Built on
+    the device from the per-cloud values (a host-side expansion meant a
+    row-sized pageable copy on every forward pass)."""
     import numpy as np
     qo = np.asarray(rows_off, dtype=np.int64)
     ro = np.asarray(offsets, dtype=np.int64)
-    counts = torch.from_numpy(np.diff(qo))
-    return torch.repeat_interleave(torch.from_numpy(ro[:-1]), counts).to(device)
+    base = torch.as_tensor(ro[:-1].astype(np.int32)).to(device, non_blocking=True)
+    counts = torch.as_tensor(np.diff(qo)).to(device, non_blocking=True)
+    return torch.repeat_interleave(base, counts, output_size=int(qo[-1]))
 
 
 class _KnnDist2Batched(torch.autograd.Function):
@@ -92,7 +95,7 @@ class _KnnDist2Batched(torch.autograd.Function):
         s = sources.detach().contiguous()
         idx, d2 = knnjoin_batched(q, q_offsets, s, r_offsets, k, squared=True)
         # indices relative to each cloud -> rows of the concatenated sources
-        base = _cloud_base(r_offsets, q_offsets, q.device).to(torch.int32)
+        base = _cloud_base(r_offsets, q_offsets, q.device)
         gidx = torch.where(idx >= 0, idx + base[:, None], idx)
         ctx.save_for_backward(q, s, gidx)
         ctx.mark_non_differentiable(idx)
