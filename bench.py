@@ -618,7 +618,9 @@ def form_batching(torch, dev, flush, steps):
     pts, off = data.ellipsoid_clouds()
     x = torch.from_numpy(pts).to(dev)
     mq, kb = x.shape[0], 16
-    g = BatchedJoinGraph(off, d=3, k=kb)
+    # one representative draw per cloud (best of 10 draws: 75.9 against 74.5
+    # ms, same evaluations and sets), for the per-cloud calls as well
+    g = BatchedJoinGraph(off, d=3, k=kb, rep_trials=1)
     g(x)
     torch.cuda.synchronize(dev)
     ms_b = _time_steps(torch, dev, lambda: g(x), steps, flush)
@@ -629,7 +631,7 @@ def form_batching(torch, dev, flush, steps):
 
     def per_cloud():
         for a0, a1 in bounds:
-            ks.knnjoin(x[a0:a1], None, kb, out=(oi[a0:a1], od[a0:a1]))
+            ks.knnjoin(x[a0:a1], None, kb, rep_trials=1, out=(oi[a0:a1], od[a0:a1]))
     ms_p = _time_steps(torch, dev, per_cloud, 1, flush)
     same_b = (torch.sort(oi, 1)[0] == torch.sort(bi, 1)[0]).all(1).float().mean().item()
     bi, bd = bi.cpu().numpy(), bd.cpu().numpy()

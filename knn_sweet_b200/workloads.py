@@ -67,7 +67,8 @@ def main(argv=None):
         pts, off = data.ellipsoid_clouds(nclouds=512 if small else 4096)
         x = torch.from_numpy(pts).cuda()
         for _ in range(a.repeat):
-            _, _, st = knnjoin_batched(x, off, k=16, autotune=not small, stats=True)
+            _, _, st = knnjoin_batched(x, off, k=16, rep_trials=1, autotune=not small,
+                                       stats=True)
         print(f"{a.workload} clouds={len(off) - 1} points={x.shape[0]}: total "
               f"{st.ms_total:.2f} ms (build {st.ms_build:.2f}, search {st.ms_search:.2f})",
               flush=True)
