@@ -43,6 +43,17 @@ namespace {
 
 // Optional phase timers (build with -DKNN_TILE_PROFILE=1): thread 0 of every
 // CTA adds the clock cycles between its barriers to tile_prof[phase].
+// Clusters in the first batch (they tighten the bounds before the rest of the
+// list is decided) and the growth of a row's compaction limit after a
+// compaction (GROW / 2 times the kept pairs, plus 32).
+#ifndef KNN_TILE_FIRST
+#define KNN_TILE_FIRST 4
+#endif
+// (first batch 2 / 4 / 8: C3 search 10.5 / 11.1 / 11.2 ms, C2 11.9 / 4.2 /
+// 4.6 ms; growth 3 / 4 / 6: C2 4.29 / 4.24 / 4.13-4.16 ms, C3 unchanged)
+#ifndef KNN_TILE_GROW
+#define KNN_TILE_GROW 6
+#endif
 #ifndef KNN_TILE_PROFILE
 #define KNN_TILE_PROFILE 0
 #endif
@@ -445,12 +456,13 @@ __global__ void __launch_bounds__(NT, NT == kTM ? 4 : 2)
         n = kept;
         tau = fminf(tau, uk);
         th_q = fminf(th_q, sqrtf(uk) * (1.0f + tol));
-        lim = min(cap - kTN, 2 * kept + 32);
+        lim = min(cap - kTN, kept * KNN_TILE_GROW / 2 + 32);
         if (kept > cap - kTN) ovf = true;
       }
     };
-    // the first batch holds the four nearest clusters only: they tighten the
+    // the first batch holds the nearest clusters only: they tighten the
     // bounds before the rest of the list is decided
+    const int nfirst = min(KNN_TILE_FIRST, nl);
     for (int jb = 0, nb = 0; jb < nl && ok; jb += nb) {
 #if KNN_CHUNK_EXIT
       // the rest of the list is prunable for every query of the tile: its
@@ -466,7 +478,7 @@ __global__ void __launch_bounds__(NT, NT == kTM ? 4 : 2)
         if (__syncthreads_and(done)) break;
       }
 #endif
-      nb = jb == 0 ? min(4, nl) : min(kTN, nl - jb);
+      nb = jb == 0 ? nfirst : min(kTN, nl - jb);
       stage_tile<NT>(
           sb, sc, KD, d, dp4,
           [&](int r) -> const float4 * {
