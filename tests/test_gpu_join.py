@@ -187,3 +187,29 @@ def test_full_size_skin_selfjoin_properties(cuda_device, oracle):
     oi, od = oracle.bruteforce_f64(x, x, 200, qrows=rows)
     assert_matches(idx[rows], dist[rows], oi, od, exact=True)
     assert st.dist_evals < 0.05 * st.pairs_total
+
+
+def test_host_calls_from_several_threads(cuda_device):
+    """Host-buffer joins keep two streams per calling thread: joins issued from
+    several threads at once (each with its own chunked copy-back) return what
+    the same joins return one at a time."""
+    import threading
+    xs = [data.skin_like(40000, seed=70 + i) for i in range(4)]
+    want = [knnjoin(x, None, 64) for x in xs]
+    got = [None] * len(xs)
+    errors = []
+
+    def run(i):
+        try:
+            for _ in range(3):
+                got[i] = knnjoin(xs[i], None, 64)
+        except Exception as e:  # reported below
+            errors.append(e)
+    threads = [threading.Thread(target=run, args=(i,)) for i in range(len(xs))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for w, g in zip(want, got):
+        assert np.array_equal(w[0], g[0]) and np.array_equal(w[1], g[1])
