@@ -112,11 +112,14 @@ def test_empty_reference_set(cuda_device):
     assert (idx == -1).all() and np.isinf(dist).all()
 
 
-def test_all_identical_points(cuda_device):
+@pytest.mark.parametrize("k", [64, 200, 600])
+def test_all_identical_points(cuda_device, k):
+    # every distance equal: the compactions' bound is the common value, the
+    # end-of-query sort leaves the binned path (one bin) for the network
     x = np.full((5000, 3), 7.0, np.float32)
-    idx, dist = knnjoin(x, None, 64)
+    idx, dist = knnjoin(x, None, k)
     assert (dist == 0).all()
-    assert (idx == np.arange(64)[None, :]).all()
+    assert (idx == np.arange(k)[None, :]).all()
 
 
 def test_deterministic_and_apis_agree(cuda_device):
